@@ -1,0 +1,416 @@
+#!/usr/bin/env python
+"""Benchmark of the IF-RK4 pseudo-spectral step on B200 (one JSON line on stdout, rank 0).
+
+Default workload (``decay2d-8192-fp32``): 2D decaying turbulence on 8192^2 in fp32 — random-
+phase vorticity (seed 0, k0 = 12, E = 0.5, E(k) ~ k^4 exp(-2 (k/k0)^2)), nu = 2e-6, 2/3
+dealiasing, CFL 0.5 with dt re-evaluated every 10 steps, as ``simulate.run`` does.  A step is
+one IF-RK4 step (4 stages x [C2R, phys, R2C, post]) of that run; the CFL reductions every 10
+steps are inside the timed region.  Synthetic data only; every field (268 MB) is larger than
+L2 (126 MB), so no L2 flush is needed between steps.
+
+Reported beside the throughput (Mpts/s = n^2 / t_step):
+  * pct_fft_roofline — the reference's roofline (src/pyspectral/benchmark.py:413-443):
+    (4 t_fft_stage + pointwise_bytes / B_copy) / t_step, with t_fft_stage the standalone
+    batched cuFFT C2R+R2C time of one stage measured here and B_copy the copy bandwidth
+    measured here;
+  * roofline — the engine's dominant own kernel (the post kernel) against measured HBM peak;
+  * cpu_baseline — the fp64/fp32 NumPy/SciPy oracle timed on this host's cores;
+  * e2e — the same run through the public API from a host state to a host state.
+
+``--impl reference`` times the reference algorithm's CPU implementation (the oracle port of
+pyspectral's NumpySolver) on the same workload instead, on rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # the decaying-turbulence headline: 8192^2 fp32, CFL 0.5, 200 steps in the full run
+    "decay2d-8192-fp32": dict(n=8192, dim=2, dtype="float32", nu=2e-6, form="basdevant",
+                              ic="random_phase", k0=12.0, seed=0, energy=0.5, cfl=0.5),
+    # plain 2D Taylor-Green: 256^2 fp64, nu=1e-2, fixed dt=1e-3
+    "tgv2d-256-fp64": dict(n=256, dim=2, dtype="float64", nu=1e-2, form="basdevant",
+                           ic="tgv2d", dt=1e-3),
+    # 3D Taylor-Green Re=1600, 512^3 fp32, CFL 0.5
+    "tgv3d-512-fp32-rotational": dict(n=512, dim=3, dtype="float32", nu=1 / 1600,
+                                      form="rotational", ic="tgv3d", cfl=0.5),
+    "tgv3d-512-fp32-basdevant": dict(n=512, dim=3, dtype="float32", nu=1 / 1600,
+                                     form="basdevant", ic="tgv3d", cfl=0.5),
+}
+PUBLISHED_MPTS = {"decay2d-8192-fp32": 547.0}  # reference, RTX 3070 Laptop, fused-inplace
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ----------------------------------------------------------------------------- helpers
+def dist_env() -> tuple[int, int, int]:
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def make_config(w: dict):
+    from pyspectral_b200 import Config
+
+    return Config(n=w["n"], dim=w["dim"], nu=w["nu"], dtype=w["dtype"], form=w["form"])
+
+
+def make_ic(w: dict):
+    from pyspectral_b200 import initial
+
+    if w["ic"] == "random_phase":
+        return initial.random_phase_2d(w["n"], k0=w["k0"], seed=w["seed"], energy=w["energy"])
+    if w["ic"] == "tgv2d":
+        return initial.to_spectral(initial.taylor_green_2d(w["n"]), 2)
+    return initial.to_spectral(initial.taylor_green_3d(w["n"]), 3)
+
+
+def traffic_model(n: int, dim: int, form: str, dtype: str) -> dict:
+    """Minimal bytes per step (src/pyspectral/benchmark.py:43-55): every FFT reads and writes
+    its data once, phys reads/writes each physical field once, the spectral kernel reads the
+    transformed products, state and accumulator and writes accumulator/state and next inputs."""
+    from pyspectral_b200.config import fft_split
+
+    sr = 8 if dtype == "float64" else 4
+    sc = 2 * sr
+    npts = float(n) ** dim
+    nmodes = float(n) ** (dim - 1) * (n // 2 + 1)
+    ni, nf = fft_split(dim, form)
+    ncomp = 1 if dim == 2 else 3
+    fft = 4 * (ni + nf) * (nmodes * sc + npts * sr)
+    phys = 4 * (ni + nf) * npts * sr
+    post = (4 * (nf + ncomp + ni) + 7 * ncomp) * nmodes * sc
+    return {"fft_bytes": fft, "pointwise_bytes": phys + post, "total_bytes": fft + phys + post,
+            "points": npts, "modes": nmodes, "ffts_per_step": 4 * (ni + nf)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:  # noqa: BLE001
+            pass
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples every 200 ms while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int) -> None:
+        self.index = index
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self) -> None:
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:  # noqa: BLE001
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:  # noqa: BLE001
+            self.proc.kill()
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                power.append(float(r[3]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, r[5:9], strict=False):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "power_w_max": max(power), "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def event_time_ms(fn, reps: int) -> float:
+    """Median CUDA-event time of fn() on the current stream."""
+    import torch
+
+    ts = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.median(ts)
+
+
+def copy_bandwidth_gbs(nbytes: int = 1 << 30) -> float:
+    """Device copy bandwidth (read + write counted), best of 10 (benchmark.py:99-116)."""
+    import torch
+
+    a = torch.empty(nbytes // 4, dtype=torch.float32, device="cuda")
+    b = torch.empty_like(a)
+    for _ in range(3):
+        b.copy_(a)
+    best = min(event_time_ms(lambda: b.copy_(a), 1) for _ in range(10))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * nbytes / (best * 1e-3) / 1e9
+
+
+def run_workload(s, w: dict, nsteps: int) -> None:
+    from pyspectral_b200.simulate import run_steps
+
+    if "dt" in w:
+        s.advance(nsteps, w["dt"])
+    else:
+        run_steps(s, nsteps, cfl=w["cfl"], dt_max=0.05, cfl_every=10)
+
+
+# ----------------------------------------------------------------------------- CPU side
+def time_oracle(w: dict, warmup: int, steps: int) -> dict:
+    """The oracle port of the reference's NumpySolver on this host (all cores via
+    scipy.fft workers=-1 for large grids): seconds per IF-RK4 step of the workload."""
+    from oracle.numpy_oracle import OracleDiagnostics, OracleSolver
+
+    ic = make_ic(w)
+    s = OracleSolver(w["n"], w["dim"], nu=w["nu"], dtype=w["dtype"], form=w["form"])
+    s.set_state(ic)
+    if "dt" in w:
+        dt = w["dt"]
+    else:
+        umax = OracleDiagnostics(w["n"], w["dim"]).max_velocity_sum(s.get_state())
+        dt = min(0.05, w["cfl"] * (2 * math.pi / w["n"]) / umax)
+    for _ in range(warmup):
+        s.step(dt)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.step(dt)
+    sec = (time.perf_counter() - t0) / steps
+    return {"sec_per_step": sec, "mpts": float(w["n"]) ** w["dim"] / sec / 1e6,
+            "cores": os.cpu_count() or 1}
+
+
+def reference_arm(args, w: dict) -> int:
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    warm = min(args.warmup, 1)
+    steps = max(1, min(args.steps, 3))
+    r = time_oracle(w, warm, steps)
+    sample = (f"{steps} IF-RK4 step(s) of the {args.workload} workload after {warm} warm-up "
+              f"step(s); NumPy + scipy.fft (pocketfft) with workers=-1 on {r['cores']} host "
+              f"threads; oracle port of pyspectral NumpySolver")
+    line = {
+        "metric": "Mpts/s/RK4 step", "value": r["mpts"], "unit": "Mpts/s", "impl": "reference",
+        "n_gpus": world, "steps": steps, "warmup": warm, "ms_per_step": r["sec_per_step"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if w["dtype"] == "float32" else "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "n": w["n"], "dim": w["dim"], "form": w["form"],
+                   "nu": w["nu"], "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": r["mpts"], "unit": "Mpts/s", "cores": r["cores"],
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": r["mpts"], "unit": "Mpts/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- GPU side
+def ours(args, w: dict) -> int:
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+
+    def barrier() -> None:
+        if pg is not None:
+            pg.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if pg is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    from pyspectral_b200.registry import make_solver
+
+    cfg = make_config(w)
+    ic = make_ic(w)
+    s = make_solver(args.variant, cfg)
+    s.set_state(ic)
+    run_workload(s, w, args.warmup)
+    torch.cuda.synchronize()
+    barrier()
+
+    # ---- timed region: K steps of the run on device-resident state
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = s.kernel_launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier()
+    ev0.record()
+    run_workload(s, w, args.steps)
+    ev1.record()
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = s.kernel_launches - l0
+    t_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    ms_step = t_ms / args.steps
+    npts = float(w["n"]) ** w["dim"]
+    value = world * npts / (ms_step * 1e-3) / 1e6
+
+    # ---- end to end through the public API: host state in, K steps, host state out
+    s2 = make_solver(args.variant, cfg)
+    s2.set_state(ic)  # first load allocates the pinned staging buffer; not timed
+    run_workload(s2, w, 1)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    s2.set_state(ic)
+    run_workload(s2, w, args.steps)
+    out = s2.get_state()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * npts * args.steps / e2e_s / 1e6
+    state_bytes = s2.u0.nbytes
+    cfl_reads = math.ceil(args.steps / 10) * 24 if "dt" not in w else 0
+    del s2, out
+    torch.cuda.empty_cache()
+
+    # ---- per-phase device times (state garbage afterwards: nothing reads it)
+    def fft_stage() -> None:
+        s.run_phase(0)
+        s.run_phase(2)
+
+    t_fft_stage = event_time_ms(fft_stage, 15)
+    t_phys = event_time_ms(lambda: s.run_phase(1), 15)
+    t_post = event_time_ms(lambda: s.run_phase(3, 1), 15)
+    bcopy = copy_bandwidth_gbs()
+    tm = traffic_model(w["n"], w["dim"], w["form"], w["dtype"])
+    t_roof_ms = 4 * t_fft_stage + tm["pointwise_bytes"] / (bcopy * 1e9) * 1e3
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    sc = 16 if w["dtype"] == "float64" else 8
+    ncomp = 1 if w["dim"] == 2 else 3
+    ninv, nfwd = s.n_inv, s.n_fwd
+    # post kernel of a middle stage: reads nfwd products + state + accumulator, writes the
+    # accumulator and the ninv next-stage inputs
+    post_bytes = (nfwd + 2 * ncomp + ncomp + ninv) * tm["modes"] * sc
+    achieved = post_bytes / (t_post * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get(args.workload, {}).get("post_stage1")
+        except Exception:  # noqa: BLE001
+            traffic = None
+
+    line = {
+        "metric": "Mpts/s/RK4 step", "value": value, "unit": "Mpts/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": (value / PUBLISHED_MPTS[args.workload]
+                        if args.workload in PUBLISHED_MPTS and world == 1 else None),
+        "dtype": "f32" if w["dtype"] == "float32" else "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "n": w["n"], "dim": w["dim"], "form": w["form"],
+                   "nu": w["nu"], "variant": args.variant, "cfl": w.get("cfl"),
+                   "dt": w.get("dt"), "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (268 MB per field), no flush"
+                         if w["n"] >= 4096 else "working set fits in L2"},
+        "pct_fft_roofline": 100.0 * t_roof_ms / ms_step,
+        "fft_roofline": {"t_fft_stage_ms": t_fft_stage, "t_roofline_step_ms": t_roof_ms,
+                         "copy_bw_gbs": bcopy, "pointwise_bytes": tm["pointwise_bytes"],
+                         "model_bytes_per_step": tm["total_bytes"],
+                         "effective_gbs": tm["total_bytes"] / (ms_step * 1e-3) / 1e9,
+                         "t_phys_ms": t_phys, "t_post_ms": t_post},
+        "roofline": {"kernel": "k_post2d<stage 1>" if w["dim"] == 2 else "k_post3d<stage 1>",
+                     "bound": "hbm", "achieved": achieved,
+                     "peak": hbm or FALLBACK_HBM_GBS, "unit": "GB/s",
+                     "frac": achieved / (hbm or FALLBACK_HBM_GBS),
+                     "peak_source": "measured" if hbm else "fallback",
+                     "algorithmic_bytes_per_launch": post_bytes, "traffic": traffic},
+        "e2e": {"value": e2e_value, "unit": "Mpts/s",
+                "h2d_bytes_per_step": state_bytes / args.steps,
+                "d2h_bytes_per_step": (state_bytes + cfl_reads) / args.steps,
+                "what": "set_state(host) + K steps + get_state(host), wall clock"},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = time_oracle(w, 1, 1)
+        line["cpu_baseline"] = {
+            "value": r["mpts"], "unit": "Mpts/s", "cores": r["cores"], "kind": "port",
+            "sample": f"1 IF-RK4 step of {args.workload} after 1 warm-up step; oracle port of "
+                      f"pyspectral NumpySolver, scipy.fft workers=-1"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def main(argv: list[str] | None = None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="decay2d-8192-fp32", choices=sorted(WORKLOADS))
+    ap.add_argument("--variant", default="b200/fused-inplace-graph")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.impl == "ours":
+        args.warmup = max(args.warmup, 3)  # at least 3 untimed warm-up steps
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return reference_arm(args, w)
+    return ours(args, w)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,163 @@
+/*
+ * spectral_b200.h — C ABI of libspectral_b200.so, the B200 (sm_100a) engine for the Lawson
+ * integrating-factor RK4 (IF-RK4) pseudo-spectral Navier-Stokes step on a periodic [0,2pi)^d box.
+ *
+ * The reference (pyspectral) drives its hot path from Python: the backend class
+ * `CupyCudaSolver` (src/pyspectral/backends/cupy_cuda.py) owns CuPy buffers, cuFFT plans and
+ * NVRTC kernels.  This header is the boundary that replaces that class's device work: a Python
+ * (ctypes) / cgo / JNI caller binds plain device pointers and a stream and calls these entry points.
+ *
+ * Conventions
+ *   - Every function returns an int status: SP_OK (0) or a negative sp_status; the message of
+ *     the last failure is returned by sp_last_error(handle) (or sp_create_error() when creation
+ *     failed).  No C++ exception crosses this boundary.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).  All device work
+ *     is enqueued on it; functions that return host values synchronise that stream.
+ *   - Device memory is owned by the caller.  sp_query_sizes() says how many bytes each buffer
+ *     needs; sp_bind() hands them over.  The library allocates nothing on the device itself
+ *     except what cuFFT plan creation reserves internally (plans run with auto-allocation off
+ *     and use the caller's `fft_workspace`).
+ *   - Spectral layout (all precisions): r2c layout of numpy.fft.rfftn, shape (n, n/2+1) in 2D and
+ *     (n, n, n/2+1) per component in 3D, row-major, unnormalised forward convention.  The state
+ *     buffer `u0` is exactly the array the reference's `state_native()` returns.
+ */
+#ifndef SPECTRAL_B200_H
+#define SPECTRAL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SP_ABI_VERSION 1
+
+typedef struct sp_solver sp_solver;
+
+enum sp_status {
+    SP_OK = 0,
+    SP_ERR_ARG = -1,         /* bad argument (size, null pointer, unsupported combination) */
+    SP_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+    SP_ERR_CUFFT = -3,       /* a cuFFT call failed */
+    SP_ERR_STATE = -4,       /* called in the wrong order (e.g. step before bind) */
+    SP_ERR_UNSUPPORTED = -5  /* option not built into this engine */
+};
+
+/* Nonlinear-term form (src/pyspectral/config.py:7-8).  2D accepts basdevant only, like the
+ * reference CUDA backend (src/pyspectral/backends/cupy_cuda.py:42-43). */
+enum sp_form { SP_FORM_BASDEVANT = 0, SP_FORM_ROTATIONAL = 1 };
+
+/* How the FFTs of a stage are executed.
+ *   SP_FFT_CUFFT       batched in-place cuFFT plans (cupy_cuda.py:100-112, variant fused-inplace)
+ *   SP_FFT_CUFFT_LEAN  single-field plans looped over the batch (cupy_cuda.py:114-128,
+ *                      variant fused-inplace-lean: cuFFT workspace of one field)            */
+enum sp_fft_mode { SP_FFT_CUFFT = 0, SP_FFT_CUFFT_LEAN = 1 };
+
+/* Indices of the array filled by sp_query_sizes(). */
+enum sp_size_index {
+    SP_SZ_MODES = 0,         /* fsc = n^(d-1) (n/2+1): complex modes per spectral field */
+    SP_SZ_NCOMP = 1,         /* state components: 1 (2D vorticity) or 3 (3D velocity) */
+    SP_SZ_NWORK = 2,         /* complex work fields W: max(inverse, forward) FFT batch */
+    SP_SZ_NINV = 3,          /* inverse FFTs per stage (config.py:84-92) */
+    SP_SZ_NFWD = 4,          /* forward FFTs per stage */
+    SP_SZ_STATE_BYTES = 5,   /* bytes of u0 (== bytes of acc) */
+    SP_SZ_WORK_BYTES = 6,    /* bytes of W */
+    SP_SZ_AUX_BYTES = 7,     /* bytes of the aux block: parameters, IF table, reduction scratch */
+    SP_SZ_FFTWS_BYTES = 8,   /* bytes of the cuFFT work area */
+    SP_SZ_NSHELL = 9,        /* number of spectrum shells (diagnostics.py:39) */
+    SP_SZ_COUNT = 10
+};
+
+/* Reduction outputs of sp_diagnostics(). */
+enum sp_diag_index {
+    SP_DIAG_ENERGY = 0,       /* <|u|^2>/2                 diagnostics.py:65-67 */
+    SP_DIAG_ENSTROPHY = 1,    /* <|omega|^2>/2             diagnostics.py:69-74 */
+    SP_DIAG_PALINSTROPHY = 2, /* <|grad omega|^2>/2 (2D)   diagnostics.py:76-82 */
+    SP_DIAG_BAND_ENERGY = 3,  /* energy in klo<=|k|<=khi   diagnostics.py:84-88 */
+    SP_DIAG_COUNT = 4
+};
+
+/* ABI version of the loaded library (SP_ABI_VERSION at build time). */
+int sp_abi_version(void);
+
+/* Create an engine for one grid.  Replaces CupyCudaSolver.__init__'s plan and kernel set-up
+ * (src/pyspectral/backends/cupy_cuda.py:40-82, plans :100-112).  Requires a CUDA device;
+ * creates the cuFFT plans (auto-allocation off).  Returns NULL on failure with *status set and
+ * the reason in sp_create_error(). */
+sp_solver* sp_create(int n, int dim, int form, int fp64, int fft_mode, int* status);
+
+/* Release plans, graphs and streams (not the caller's buffers). */
+void sp_destroy(sp_solver* s);
+
+/* Fill out[0..count) with the sp_size_index values (count <= SP_SZ_COUNT). */
+int sp_query_sizes(const sp_solver* s, int64_t* out, int count);
+
+/* Hand over caller-owned device buffers (sizes from sp_query_sizes, 256-byte aligned):
+ * u0 = state, acc = RK accumulator, work = W (FFT work fields), aux = parameter block, IF table
+ * and reduction scratch, fft_workspace = cuFFT work area.  Replaces the buffer allocation of
+ * cupy_cuda.py:53-66.  Must be called once before any stepping. */
+int sp_bind(sp_solver* s, void* u0, void* acc, void* work, void* aux, void* fft_workspace);
+
+/* Physical parameters of the linear operator L(k) (src/pyspectral/backends/base.py:114-123):
+ * viscosity nu, drag alpha on k^2 <= drag_k2 (config.py:59-62), forcing band [klo, khi]. */
+int sp_set_physics(sp_solver* s, double nu, double alpha, double drag_k2, double force_klo,
+                   double force_khi);
+
+/* Band-forcing growth rate A, honoured from the next step on (base.py:98-100). */
+int sp_set_forcing_amplitude(sp_solver* s, double amp);
+
+/* Load the state just written into u0 (CupyCudaSolver.set_state + _pre, cupy_cuda.py:134-145,
+ * kernels pre2d/pre3d of src/pyspectral/kernels/spectral.cu:93-103,164-173): dealiases u0 in
+ * place (the 2/3 mask check_state applies on the host, src/pyspectral/backends/base.py:134-139)
+ * and builds the stage-0 FFT inputs. */
+int sp_prepare(sp_solver* s, void* stream);
+
+/* Advance one IF-RK4 step of size dt (CupyCudaSolver._step + _stage, cupy_cuda.py:163-195).
+ * Parameters live in device memory, so one captured CUDA graph serves every dt and forcing
+ * amplitude (no re-capture per (dt, amp) as at cupy_cuda.py:181-195). */
+int sp_step(sp_solver* s, double dt, void* stream);
+
+/* 1 = replay each step from a CUDA graph (variant fused-inplace-graph), 0 = plain launches. */
+int sp_set_graph(sp_solver* s, int enable);
+
+/* Spectral reductions of a state array (device pointer in the u0 layout, e.g. u0 itself):
+ * writes SP_DIAG_COUNT doubles to out (host) — energy, enstrophy, palinstrophy and the energy in
+ * band_klo <= |k| <= band_khi — summed in fp64 in a fixed order.  Synchronises `stream`. */
+int sp_diagnostics(sp_solver* s, const void* state, double band_klo, double band_khi,
+                   double* out, void* stream);
+
+/* sum_i max|u_i| in physical space of a state array (Diagnostics.max_velocity_sum,
+ * src/pyspectral/diagnostics.py:99-109); out_per_comp (host, 3 doubles, may be NULL) receives
+ * each component's max.  Uses the RK accumulator as scratch (it is dead between steps).
+ * Synchronises `stream`. */
+int sp_max_velocity(sp_solver* s, const void* state, double* out_sum, double* out_per_comp,
+                    void* stream);
+
+/* Shell-summed energy spectrum E(k), k = 0..nshell-1 (Diagnostics.spectrum,
+ * src/pyspectral/diagnostics.py:90-97), written to out (host, nshell doubles). */
+int sp_spectrum(sp_solver* s, const void* state, double* out, int nshell, void* stream);
+
+/* Run one phase of one stage by itself (for per-phase timing and profiling):
+ * phase 0 = batched inverse FFT, 1 = physical-space kernel, 2 = batched forward FFT,
+ * 3 = spectral kernel of RK stage `stage` (0..3) using the parameters of the last step.
+ * Phases 0+2 back to back are the standalone "FFT ceiling" of one stage
+ * (src/pyspectral/benchmark.py:145-214). */
+int sp_run_phase(sp_solver* s, int phase, int stage, void* stream);
+
+/* Number of this library's own kernels launched through the handle so far (a graph replay
+ * counts the kernels it contains; cuFFT's kernels are not counted).  -1 for a null handle.
+ * No reference counterpart: instrumentation for the benchmark. */
+int64_t sp_kernel_launches(const sp_solver* s);
+
+/* Message of the last failure on this handle (never NULL). */
+const char* sp_last_error(const sp_solver* s);
+
+/* Message of the last sp_create failure in this thread (never NULL). */
+const char* sp_create_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPECTRAL_B200_H */

@@ -1,0 +1,90 @@
+"""ctypes binding of libspectral_b200.so (declarations in include/spectral_b200.h).
+
+The library is loaded from this package directory only.  A missing library or a missing CUDA
+device raises :class:`BackendUnavailable` — there is no other implementation to fall back to.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+from typing import Any
+
+from pyspectral_b200.base import BackendUnavailable
+
+LIB_PATH = Path(__file__).resolve().parent / "libspectral_b200.so"
+
+# status codes (enum sp_status)
+SP_OK = 0
+STATUS_NAMES = {0: "SP_OK", -1: "SP_ERR_ARG", -2: "SP_ERR_CUDA", -3: "SP_ERR_CUFFT",
+                -4: "SP_ERR_STATE", -5: "SP_ERR_UNSUPPORTED"}
+# enum sp_form / sp_fft_mode
+FORM_CODES = {"basdevant": 0, "rotational": 1}
+FFT_CUFFT, FFT_CUFFT_LEAN = 0, 1
+# enum sp_size_index
+SZ_MODES, SZ_NCOMP, SZ_NWORK, SZ_NINV, SZ_NFWD = 0, 1, 2, 3, 4
+SZ_STATE_BYTES, SZ_WORK_BYTES, SZ_AUX_BYTES, SZ_FFTWS_BYTES, SZ_NSHELL, SZ_COUNT = 5, 6, 7, 8, 9, 10
+
+_vp, _i, _d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+_dp = ctypes.POINTER(ctypes.c_double)
+
+# name -> (restype, argtypes); the exported C ABI
+SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
+    "sp_abi_version": (_i, []),
+    "sp_create": (_vp, [_i, _i, _i, _i, _i, ctypes.POINTER(_i)]),
+    "sp_destroy": (None, [_vp]),
+    "sp_query_sizes": (_i, [_vp, ctypes.POINTER(ctypes.c_int64), _i]),
+    "sp_bind": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "sp_set_physics": (_i, [_vp, _d, _d, _d, _d, _d]),
+    "sp_set_forcing_amplitude": (_i, [_vp, _d]),
+    "sp_prepare": (_i, [_vp, _vp]),
+    "sp_step": (_i, [_vp, _d, _vp]),
+    "sp_set_graph": (_i, [_vp, _i]),
+    "sp_diagnostics": (_i, [_vp, _vp, _d, _d, _dp, _vp]),
+    "sp_max_velocity": (_i, [_vp, _vp, _dp, _dp, _vp]),
+    "sp_spectrum": (_i, [_vp, _vp, _dp, _i, _vp]),
+    "sp_run_phase": (_i, [_vp, _i, _i, _vp]),
+    "sp_kernel_launches": (ctypes.c_int64, [_vp]),
+    "sp_last_error": (ctypes.c_char_p, [_vp]),
+    "sp_create_error": (ctypes.c_char_p, []),
+}
+
+_LIB: ctypes.CDLL | None = None
+
+
+def load() -> ctypes.CDLL:
+    """Load (once) and declare the library; BackendUnavailable if it is not built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not LIB_PATH.exists():
+        raise BackendUnavailable(
+            f"{LIB_PATH.name} is not built (run `python -m pyspectral_b200.build`)")
+    try:
+        lib = ctypes.CDLL(str(LIB_PATH))
+    except OSError as e:
+        raise BackendUnavailable(f"cannot load {LIB_PATH.name}: {e}") from e
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+class EngineError(RuntimeError):
+    """A call into the engine returned a non-zero status."""
+
+
+def check(lib: ctypes.CDLL, handle: int | None, status: int, what: str) -> None:
+    """Raise EngineError with the engine's message when ``status`` is not SP_OK."""
+    if status == SP_OK:
+        return
+    msg = lib.sp_last_error(handle) if handle else lib.sp_create_error()
+    text = msg.decode() if msg else ""
+    raise EngineError(f"{what} failed: {STATUS_NAMES.get(status, status)}: {text}")
+
+
+def dptr(arr: Any) -> ctypes.c_void_p:
+    """Device pointer of a torch tensor (or None)."""
+    return ctypes.c_void_p(arr.data_ptr()) if arr is not None else ctypes.c_void_p(0)

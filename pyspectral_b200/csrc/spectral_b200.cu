@@ -1,0 +1,647 @@
+// libspectral_b200: C ABI (include/spectral_b200.h) over the B200 IF-RK4 engine.
+//
+// One handle = one grid.  The host side of the reference backend (CupyCudaSolver,
+// src/pyspectral/backends/cupy_cuda.py) is re-designed here in C++:
+//   * cuFFT plans are created from C++ with auto-allocation off; their work area is a caller
+//     buffer shared by every plan of the handle (the plans only run one after another).
+//   * the per-step scalars (dt, drag and band factors) and the 1D integrating-factor table live
+//     in device memory and are refreshed with one small copy only when they change, so a single
+//     captured CUDA graph replays every step whatever dt or the forcing amplitude is.
+//   * the pointwise phases are the fused kernels of pointwise.cuh; reductions are reduce.cuh.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "spectral_b200.h"
+#include "pointwise.cuh"
+#include "reduce.cuh"
+
+using namespace sp;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+const char* cufft_name(cufftResult r) {
+    switch (r) {
+        case CUFFT_SUCCESS: return "CUFFT_SUCCESS";
+        case CUFFT_INVALID_PLAN: return "CUFFT_INVALID_PLAN";
+        case CUFFT_ALLOC_FAILED: return "CUFFT_ALLOC_FAILED";
+        case CUFFT_INVALID_TYPE: return "CUFFT_INVALID_TYPE";
+        case CUFFT_INVALID_VALUE: return "CUFFT_INVALID_VALUE";
+        case CUFFT_INTERNAL_ERROR: return "CUFFT_INTERNAL_ERROR";
+        case CUFFT_EXEC_FAILED: return "CUFFT_EXEC_FAILED";
+        case CUFFT_SETUP_FAILED: return "CUFFT_SETUP_FAILED";
+        case CUFFT_INVALID_SIZE: return "CUFFT_INVALID_SIZE";
+        case CUFFT_UNALIGNED_DATA: return "CUFFT_UNALIGNED_DATA";
+        case CUFFT_INVALID_DEVICE: return "CUFFT_INVALID_DEVICE";
+        case CUFFT_NO_WORKSPACE: return "CUFFT_NO_WORKSPACE";
+        case CUFFT_NOT_IMPLEMENTED: return "CUFFT_NOT_IMPLEMENTED";
+        case CUFFT_NOT_SUPPORTED: return "CUFFT_NOT_SUPPORTED";
+        default: return "CUFFT_UNKNOWN_ERROR";
+    }
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+struct sp_solver {
+    // grid
+    int n = 0, dim = 0, form = 0, fp64 = 0, fft_mode = 0;
+    int nh = 0, ncomp = 0, nwork = 0, ninv = 0, nfwd = 0, nshell = 0;
+    uint32_t fsc = 0, fsr = 0;
+    size_t rsize = 0;  // bytes of one real
+    // caller buffers
+    void *u0 = nullptr, *acc = nullptr, *W = nullptr, *aux = nullptr, *fftws = nullptr;
+    bool bound = false;
+    // aux sub-blocks
+    size_t off_params = 0, off_tab = 0, off_partials = 0, off_umax = 0, off_out = 0, off_spec = 0;
+    size_t aux_bytes = 0;
+    // cuFFT
+    cufftHandle plan_inv = 0, plan_fwd = 0, plan_c2r1 = 0;
+    bool have_inv = false, have_fwd = false, have_c2r1 = false;
+    size_t ws_bytes = 0;
+    // physics and the host copy of the device parameter block
+    double nu = 0, alpha = 0, drag_k2 = 1e30, klo = 0, khi = 0, amp = 0;
+    bool tab_valid = false, params_valid = false;
+    double tab_dt = 0, tab_nu = 0;
+    std::vector<unsigned char> host_params, host_tab;
+    // own kernel launches issued so far (graph replays count their captured kernels)
+    int64_t launches = 0;
+    int64_t graph_kernels = 0;
+    // graph
+    bool graph_on = false;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    // last error
+    std::string err;
+
+    void* params_dev() const { return (char*)aux + off_params; }
+    void* tab_dev() const { return (char*)aux + off_tab; }
+    double* partials_dev() const { return (double*)((char*)aux + off_partials); }
+    unsigned long long* umax_dev() const { return (unsigned long long*)((char*)aux + off_umax); }
+    double* out_dev() const { return (double*)((char*)aux + off_out); }
+    double* spec_dev() const { return (double*)((char*)aux + off_spec); }
+};
+
+namespace {
+
+int fail(sp_solver* s, int code, const char* what, const char* why) {
+    if (s) {
+        s->err = std::string(what) + ": " + why;
+    }
+    return code;
+}
+
+#define SP_CUDA(call)                                                                \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) return fail(s, SP_ERR_CUDA, #call, cudaGetErrorString(e_)); \
+    } while (0)
+#define SP_CUFFT(call)                                                                \
+    do {                                                                              \
+        cufftResult r_ = (call);                                                      \
+        if (r_ != CUFFT_SUCCESS) return fail(s, SP_ERR_CUFFT, #call, cufft_name(r_)); \
+    } while (0)
+#define SP_CHECK_BOUND(s)                                                             \
+    do {                                                                              \
+        if (!(s)) return SP_ERR_ARG;                                                  \
+        if (!(s)->bound) return fail((s), SP_ERR_STATE, "engine", "sp_bind was not called"); \
+    } while (0)
+
+unsigned grid_for(uint64_t items, int block) { return (unsigned)((items + block - 1) / block); }
+
+// ---------------------------------------------------------------------------- parameters
+// Integrating-factor table and step scalars in the real type, computed in fp64 on the host
+// exactly like if_table / if_scalars (src/pyspectral/backends/_fused_common.py:10-19) and the
+// band on/off rule of cupy_cuda.py:156-159.
+template <typename T>
+void fill_params(sp_solver* s, double dt, std::vector<unsigned char>& out) {
+    StepParams<T> p;
+    p.dt = (T)dt;
+    p.ea1 = (T)std::exp(-s->alpha * dt);
+    p.eah = (T)std::exp(-s->alpha * 0.5 * dt);
+    p.eb1 = (T)std::exp(s->amp * dt);
+    p.ebh = (T)std::exp(s->amp * 0.5 * dt);
+    bool band_on = s->amp != 0.0;
+    p.klo2 = band_on ? (T)(s->klo * s->klo) : (T)1;
+    p.khi2 = band_on ? (T)(s->khi * s->khi) : (T)0;
+    p.ka2 = (T)s->drag_k2;
+    p.scale = (T)(1.0 / std::pow((double)s->n, (double)s->dim));
+    out.resize(sizeof(p));
+    std::memcpy(out.data(), &p, sizeof(p));
+}
+
+template <typename T>
+void fill_table(sp_solver* s, double dt, std::vector<unsigned char>& out) {
+    std::vector<T> t(2 * (size_t)s->nh);
+    for (int m = 0; m < s->nh; ++m) {
+        double mm = (double)m;
+        t[m] = (T)std::exp(-s->nu * mm * mm * dt);
+        t[s->nh + m] = (T)std::exp(-s->nu * mm * mm * 0.5 * dt);
+    }
+    out.resize(t.size() * sizeof(T));
+    std::memcpy(out.data(), t.data(), out.size());
+}
+
+int upload_params(sp_solver* s, double dt, cudaStream_t st) {
+    if (!s->tab_valid || s->tab_dt != dt || s->tab_nu != s->nu) {
+        if (s->fp64) fill_table<double>(s, dt, s->host_tab);
+        else fill_table<float>(s, dt, s->host_tab);
+        // pageable source: the call returns once the bytes are staged, so host_tab may change
+        SP_CUDA(cudaMemcpyAsync(s->tab_dev(), s->host_tab.data(), s->host_tab.size(),
+                                cudaMemcpyHostToDevice, st));
+        s->tab_valid = true;
+        s->tab_dt = dt;
+        s->tab_nu = s->nu;
+    }
+    std::vector<unsigned char> p;
+    if (s->fp64) fill_params<double>(s, dt, p);
+    else fill_params<float>(s, dt, p);
+    if (!s->params_valid || p != s->host_params) {
+        s->host_params = p;
+        SP_CUDA(cudaMemcpyAsync(s->params_dev(), s->host_params.data(), s->host_params.size(),
+                                cudaMemcpyHostToDevice, st));
+        s->params_valid = true;
+    }
+    return SP_OK;
+}
+
+// ---------------------------------------------------------------------------- FFTs
+int make_plan(sp_solver* s, bool inverse, int batch, cufftHandle* plan, size_t* ws) {
+    long long shape[3], cemb[3], remb[3];
+    for (int i = 0; i < s->dim; ++i) {
+        shape[i] = s->n;
+        cemb[i] = s->n;
+        remb[i] = s->n;
+    }
+    cemb[s->dim - 1] = s->nh;
+    remb[s->dim - 1] = 2LL * s->nh;
+    SP_CUFFT(cufftCreate(plan));
+    SP_CUFFT(cufftSetAutoAllocation(*plan, 0));
+    long long cdist = s->fsc, rdist = 2LL * s->fsc;
+    if (inverse) {
+        SP_CUFFT(cufftMakePlanMany64(*plan, s->dim, shape, cemb, 1, cdist, remb, 1, rdist,
+                                     s->fp64 ? CUFFT_Z2D : CUFFT_C2R, batch, ws));
+    } else {
+        SP_CUFFT(cufftMakePlanMany64(*plan, s->dim, shape, remb, 1, rdist, cemb, 1, cdist,
+                                     s->fp64 ? CUFFT_D2Z : CUFFT_R2C, batch, ws));
+    }
+    return SP_OK;
+}
+
+int exec_c2r(sp_solver* s, cufftHandle plan, void* field, cudaStream_t st) {
+    SP_CUFFT(cufftSetStream(plan, st));
+    if (s->fp64) {
+        SP_CUFFT(cufftExecZ2D(plan, (cufftDoubleComplex*)field, (cufftDoubleReal*)field));
+    } else {
+        SP_CUFFT(cufftExecC2R(plan, (cufftComplex*)field, (cufftReal*)field));
+    }
+    return SP_OK;
+}
+
+int exec_r2c(sp_solver* s, cufftHandle plan, void* field, cudaStream_t st) {
+    SP_CUFFT(cufftSetStream(plan, st));
+    if (s->fp64) {
+        SP_CUFFT(cufftExecD2Z(plan, (cufftDoubleReal*)field, (cufftDoubleComplex*)field));
+    } else {
+        SP_CUFFT(cufftExecR2C(plan, (cufftReal*)field, (cufftComplex*)field));
+    }
+    return SP_OK;
+}
+
+size_t field_bytes(const sp_solver* s) { return (size_t)s->fsc * 2 * s->rsize; }
+
+int fft_inverse(sp_solver* s, cudaStream_t st) {
+    if (s->fft_mode == SP_FFT_CUFFT) return exec_c2r(s, s->plan_inv, s->W, st);
+    for (int i = 0; i < s->ninv; ++i) {
+        int r = exec_c2r(s, s->plan_inv, (char*)s->W + i * field_bytes(s), st);
+        if (r) return r;
+    }
+    return SP_OK;
+}
+
+int fft_forward(sp_solver* s, cudaStream_t st) {
+    if (s->fft_mode == SP_FFT_CUFFT) return exec_r2c(s, s->plan_fwd, s->W, st);
+    for (int i = 0; i < s->nfwd; ++i) {
+        int r = exec_r2c(s, s->plan_fwd, (char*)s->W + i * field_bytes(s), st);
+        if (r) return r;
+    }
+    return SP_OK;
+}
+
+// ---------------------------------------------------------------------------- kernels
+template <typename T>
+int launch_pre(sp_solver* s, cudaStream_t st) {
+    auto* u0 = (cplx<T>*)s->u0;
+    auto* W = (cplx<T>*)s->W;
+    auto* P = (const StepParams<T>*)s->params_dev();
+    unsigned g = grid_for(s->fsc / 2, kBlock);
+    if (s->dim == 2) k_pre2d<T><<<g, kBlock, 0, st>>>(u0, W, s->n, s->nh, s->fsc, P);
+    else if (s->form == SP_FORM_ROTATIONAL)
+        k_pre3d<T, true><<<g, kBlock, 0, st>>>(u0, W, s->n, s->nh, s->fsc, P);
+    else k_pre3d<T, false><<<g, kBlock, 0, st>>>(u0, W, s->n, s->nh, s->fsc, P);
+    SP_CUDA(cudaGetLastError());
+    s->launches += 1;
+    return SP_OK;
+}
+
+template <typename T>
+int launch_phys(sp_solver* s, cudaStream_t st) {
+    auto* R = (T*)s->W;
+    unsigned g = grid_for(s->fsr / 4, kBlock);
+    if (s->dim == 2) k_phys2d<T><<<g, kBlock, 0, st>>>(R, s->fsr);
+    else if (s->form == SP_FORM_ROTATIONAL) k_phys3d_rot<T><<<g, kBlock, 0, st>>>(R, s->fsr);
+    else k_phys3d_basd<T><<<g, kBlock, 0, st>>>(R, s->fsr);
+    SP_CUDA(cudaGetLastError());
+    s->launches += 1;
+    return SP_OK;
+}
+
+template <typename T, int STAGE>
+void post_stage(sp_solver* s, cudaStream_t st) {
+    auto* W = (cplx<T>*)s->W;
+    auto* u0 = (cplx<T>*)s->u0;
+    auto* acc = (cplx<T>*)s->acc;
+    auto* tab = (const T*)s->tab_dev();
+    auto* P = (const StepParams<T>*)s->params_dev();
+    unsigned g = grid_for(s->fsc / 2, kBlock);
+    if (s->dim == 2)
+        k_post2d<T, STAGE><<<g, kBlock, 0, st>>>(W, u0, acc, tab, P, s->n, s->nh, s->fsc);
+    else if (s->form == SP_FORM_ROTATIONAL)
+        k_post3d<T, true, STAGE><<<g, kBlock, 0, st>>>(W, u0, acc, tab, P, s->n, s->nh, s->fsc);
+    else
+        k_post3d<T, false, STAGE><<<g, kBlock, 0, st>>>(W, u0, acc, tab, P, s->n, s->nh, s->fsc);
+}
+
+template <typename T>
+int launch_post(sp_solver* s, int stage, cudaStream_t st) {
+    switch (stage) {
+        case 0: post_stage<T, 0>(s, st); break;
+        case 1: post_stage<T, 1>(s, st); break;
+        case 2: post_stage<T, 2>(s, st); break;
+        default: post_stage<T, 3>(s, st); break;
+    }
+    SP_CUDA(cudaGetLastError());
+    s->launches += 1;
+    return SP_OK;
+}
+
+int run_pre(sp_solver* s, cudaStream_t st) {
+    return s->fp64 ? launch_pre<double>(s, st) : launch_pre<float>(s, st);
+}
+int run_phys(sp_solver* s, cudaStream_t st) {
+    return s->fp64 ? launch_phys<double>(s, st) : launch_phys<float>(s, st);
+}
+int run_post(sp_solver* s, int stage, cudaStream_t st) {
+    return s->fp64 ? launch_post<double>(s, stage, st) : launch_post<float>(s, stage, st);
+}
+
+// One IF-RK4 step: 4 x (inverse FFT -> phys -> forward FFT -> post), cupy_cuda.py:163-178.
+int run_step(sp_solver* s, cudaStream_t st) {
+    for (int stage = 0; stage < 4; ++stage) {
+        int r;
+        if ((r = fft_inverse(s, st))) return r;
+        if ((r = run_phys(s, st))) return r;
+        if ((r = fft_forward(s, st))) return r;
+        if ((r = run_post(s, stage, st))) return r;
+    }
+    return SP_OK;
+}
+
+int capture_step(sp_solver* s) {
+    if (!s->cap_stream) SP_CUDA(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
+    SP_CUDA(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int64_t before = s->launches;
+    int r = run_step(s, s->cap_stream);
+    s->graph_kernels = s->launches - before;
+    s->launches = before;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->cap_stream, &g);
+    if (r) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return fail(s, SP_ERR_CUDA, "cudaStreamEndCapture", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&s->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        s->exec = nullptr;
+        return fail(s, SP_ERR_CUDA, "cudaGraphInstantiate", cudaGetErrorString(e));
+    }
+    return SP_OK;
+}
+
+void drop_graph(sp_solver* s) {
+    if (s->exec) {
+        cudaGraphExecDestroy(s->exec);
+        s->exec = nullptr;
+    }
+}
+
+}  // namespace
+
+// ============================================================================== C ABI
+extern "C" {
+
+int sp_abi_version(void) { return SP_ABI_VERSION; }
+
+const char* sp_create_error(void) { return g_create_error.c_str(); }
+
+const char* sp_last_error(const sp_solver* s) { return s ? s->err.c_str() : "null handle"; }
+
+int64_t sp_kernel_launches(const sp_solver* s) { return s ? s->launches : -1; }
+
+sp_solver* sp_create(int n, int dim, int form, int fp64, int fft_mode, int* status) {
+    auto set = [&](int code, const std::string& why) -> sp_solver* {
+        if (status) *status = code;
+        g_create_error = why;
+        return nullptr;
+    };
+    if (dim != 2 && dim != 3) return set(SP_ERR_ARG, "dim must be 2 or 3");
+    if (n < 8 || n % 2) return set(SP_ERR_ARG, "n must be even and >= 8");
+    if (form != SP_FORM_BASDEVANT && form != SP_FORM_ROTATIONAL)
+        return set(SP_ERR_ARG, "unknown form");
+    if (dim == 2 && form != SP_FORM_BASDEVANT)
+        return set(SP_ERR_UNSUPPORTED, "2D supports the basdevant form only");
+    if (fft_mode != SP_FFT_CUFFT && fft_mode != SP_FFT_CUFFT_LEAN)
+        return set(SP_ERR_ARG, "unknown fft_mode");
+    int nh = n / 2 + 1;
+    uint64_t fsc = (uint64_t)nh * (uint64_t)n * (dim == 3 ? (uint64_t)n : 1ull);
+    if (2 * fsc >= (1ull << 32)) return set(SP_ERR_ARG, "grid too large for 32-bit indexing");
+    int ndev = 0;
+    cudaError_t ce = cudaGetDeviceCount(&ndev);
+    if (ce != cudaSuccess || ndev < 1)
+        return set(SP_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(ce));
+
+    auto* s = new sp_solver();
+    s->n = n;
+    s->dim = dim;
+    s->form = form;
+    s->fp64 = fp64 ? 1 : 0;
+    s->fft_mode = fft_mode;
+    s->nh = nh;
+    s->fsc = (uint32_t)fsc;
+    s->fsr = (uint32_t)(2 * fsc);
+    s->rsize = fp64 ? 8 : 4;
+    s->ncomp = dim == 2 ? 1 : 3;
+    if (dim == 2) { s->ninv = 2; s->nfwd = 2; }
+    else if (form == SP_FORM_ROTATIONAL) { s->ninv = 6; s->nfwd = 3; }
+    else { s->ninv = 3; s->nfwd = 5; }
+    s->nwork = s->ninv > s->nfwd ? s->ninv : s->nfwd;
+    s->nshell = (int)std::floor(std::sqrt((double)dim) * (double)(n / 2) + 0.5) + 1;
+    // aux layout
+    size_t off = 0;
+    s->off_params = off; off += align256(16 * sizeof(double));
+    s->off_tab = off; off += align256(2 * (size_t)nh * s->rsize);
+    s->off_partials = off; off += align256((size_t)kRedBlocks * 4 * sizeof(double));
+    s->off_umax = off; off += align256(4 * sizeof(unsigned long long));
+    s->off_out = off; off += align256(8 * sizeof(double));
+    s->off_spec = off; off += align256((size_t)s->nshell * sizeof(double));
+    s->aux_bytes = off;
+
+    bool lean = fft_mode == SP_FFT_CUFFT_LEAN;
+    size_t ws_inv = 0, ws_fwd = 0, ws_one = 0;
+    int r = make_plan(s, true, lean ? 1 : s->ninv, &s->plan_inv, &ws_inv);
+    if (!r) { s->have_inv = true; r = make_plan(s, false, lean ? 1 : s->nfwd, &s->plan_fwd, &ws_fwd); }
+    if (!r) s->have_fwd = true;
+    if (!r && !lean) {
+        r = make_plan(s, true, 1, &s->plan_c2r1, &ws_one);
+        if (!r) s->have_c2r1 = true;
+    }
+    if (r) {
+        std::string why = s->err;
+        sp_destroy(s);
+        return set(r, why);
+    }
+    s->ws_bytes = ws_inv > ws_fwd ? ws_inv : ws_fwd;
+    if (ws_one > s->ws_bytes) s->ws_bytes = ws_one;
+    if (status) *status = SP_OK;
+    return s;
+}
+
+void sp_destroy(sp_solver* s) {
+    if (!s) return;
+    drop_graph(s);
+    if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
+    if (s->have_inv) cufftDestroy(s->plan_inv);
+    if (s->have_fwd) cufftDestroy(s->plan_fwd);
+    if (s->have_c2r1) cufftDestroy(s->plan_c2r1);
+    delete s;
+}
+
+int sp_query_sizes(const sp_solver* s, int64_t* out, int count) {
+    if (!s || !out || count < 0 || count > SP_SZ_COUNT) return SP_ERR_ARG;
+    int64_t v[SP_SZ_COUNT];
+    v[SP_SZ_MODES] = s->fsc;
+    v[SP_SZ_NCOMP] = s->ncomp;
+    v[SP_SZ_NWORK] = s->nwork;
+    v[SP_SZ_NINV] = s->ninv;
+    v[SP_SZ_NFWD] = s->nfwd;
+    v[SP_SZ_STATE_BYTES] = (int64_t)s->ncomp * (int64_t)field_bytes(s);
+    v[SP_SZ_WORK_BYTES] = (int64_t)s->nwork * (int64_t)field_bytes(s);
+    v[SP_SZ_AUX_BYTES] = (int64_t)s->aux_bytes;
+    v[SP_SZ_FFTWS_BYTES] = (int64_t)s->ws_bytes;
+    v[SP_SZ_NSHELL] = s->nshell;
+    for (int i = 0; i < count; ++i) out[i] = v[i];
+    return SP_OK;
+}
+
+int sp_bind(sp_solver* s, void* u0, void* acc, void* work, void* aux, void* fft_workspace) {
+    if (!s) return SP_ERR_ARG;
+    if (!u0 || !acc || !work || !aux || (s->ws_bytes && !fft_workspace))
+        return fail(s, SP_ERR_ARG, "sp_bind", "null buffer");
+    for (void* p : {u0, acc, work, aux})
+        if ((uintptr_t)p % 256) return fail(s, SP_ERR_ARG, "sp_bind", "buffer not 256-byte aligned");
+    s->u0 = u0;
+    s->acc = acc;
+    s->W = work;
+    s->aux = aux;
+    s->fftws = fft_workspace;
+    if (s->ws_bytes) {
+        SP_CUFFT(cufftSetWorkArea(s->plan_inv, fft_workspace));
+        SP_CUFFT(cufftSetWorkArea(s->plan_fwd, fft_workspace));
+        if (s->have_c2r1) SP_CUFFT(cufftSetWorkArea(s->plan_c2r1, fft_workspace));
+    }
+    s->bound = true;
+    s->tab_valid = false;
+    s->params_valid = false;
+    drop_graph(s);
+    return SP_OK;
+}
+
+int sp_set_physics(sp_solver* s, double nu, double alpha, double drag_k2, double force_klo,
+                   double force_khi) {
+    if (!s) return SP_ERR_ARG;
+    s->nu = nu;
+    s->alpha = alpha;
+    s->drag_k2 = drag_k2;
+    s->klo = force_klo;
+    s->khi = force_khi;
+    return SP_OK;
+}
+
+int sp_set_forcing_amplitude(sp_solver* s, double amp) {
+    if (!s) return SP_ERR_ARG;
+    s->amp = amp;
+    return SP_OK;
+}
+
+int sp_prepare(sp_solver* s, void* stream) {
+    SP_CHECK_BOUND(s);
+    auto st = (cudaStream_t)stream;
+    // the scale lives in the parameter block: make sure it exists (dt is irrelevant here)
+    if (!s->params_valid) {
+        int r = upload_params(s, s->tab_valid ? s->tab_dt : 0.0, st);
+        if (r) return r;
+    }
+    return run_pre(s, st);
+}
+
+int sp_set_graph(sp_solver* s, int enable) {
+    if (!s) return SP_ERR_ARG;
+    s->graph_on = enable != 0;
+    if (!s->graph_on) drop_graph(s);
+    return SP_OK;
+}
+
+int sp_step(sp_solver* s, double dt, void* stream) {
+    SP_CHECK_BOUND(s);
+    auto st = (cudaStream_t)stream;
+    int r = upload_params(s, dt, st);
+    if (r) return r;
+    if (!s->graph_on) return run_step(s, st);
+    if (!s->exec && (r = capture_step(s))) return r;
+    SP_CUDA(cudaGraphLaunch(s->exec, st));
+    s->launches += s->graph_kernels;
+    return SP_OK;
+}
+
+int sp_run_phase(sp_solver* s, int phase, int stage, void* stream) {
+    SP_CHECK_BOUND(s);
+    auto st = (cudaStream_t)stream;
+    if (stage < 0 || stage > 3) return fail(s, SP_ERR_ARG, "sp_run_phase", "stage must be 0..3");
+    switch (phase) {
+        case 0: return fft_inverse(s, st);
+        case 1: return run_phys(s, st);
+        case 2: return fft_forward(s, st);
+        case 3:
+            if (!s->params_valid) return fail(s, SP_ERR_STATE, "sp_run_phase", "no step parameters yet");
+            return run_post(s, stage, st);
+        default: return fail(s, SP_ERR_ARG, "sp_run_phase", "phase must be 0..3");
+    }
+}
+
+int sp_diagnostics(sp_solver* s, const void* state, double band_klo, double band_khi,
+                   double* out, void* stream) {
+    SP_CHECK_BOUND(s);
+    if (!state || !out) return fail(s, SP_ERR_ARG, "sp_diagnostics", "null pointer");
+    auto st = (cudaStream_t)stream;
+    double norm = std::pow((double)s->n, 2.0 * s->dim);
+    double w_edge = 1.0 / norm, w_mid = 2.0 / norm;
+    unsigned g = grid_for(s->fsc, kRedThreads);
+    if (g > (unsigned)kRedBlocks) g = kRedBlocks;
+    double klo2 = band_klo * band_klo, khi2 = band_khi * band_khi;
+    if (s->fp64)
+        k_reduce_spectral<double><<<g, kRedThreads, 0, st>>>((const cplx<double>*)state, s->n, s->nh,
+                                                             s->dim, s->fsc, w_edge, w_mid, klo2,
+                                                             khi2, s->partials_dev());
+    else
+        k_reduce_spectral<float><<<g, kRedThreads, 0, st>>>((const cplx<float>*)state, s->n, s->nh,
+                                                            s->dim, s->fsc, w_edge, w_mid, klo2,
+                                                            khi2, s->partials_dev());
+    SP_CUDA(cudaGetLastError());
+    k_finish_sum<4><<<1, kRedThreads, 0, st>>>(s->partials_dev(), (int)g, 0.5, s->out_dev());
+    SP_CUDA(cudaGetLastError());
+    s->launches += 2;
+    SP_CUDA(cudaMemcpyAsync(out, s->out_dev(), 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SP_CUDA(cudaStreamSynchronize(st));
+    return SP_OK;
+}
+
+int sp_max_velocity(sp_solver* s, const void* state, double* out_sum, double* out_per_comp,
+                    void* stream) {
+    SP_CHECK_BOUND(s);
+    if (!state || !out_sum) return fail(s, SP_ERR_ARG, "sp_max_velocity", "null pointer");
+    auto st = (cudaStream_t)stream;
+    int ncomp = s->dim;  // velocity components
+    cufftHandle plan = s->fft_mode == SP_FFT_CUFFT_LEAN ? s->plan_inv : s->plan_c2r1;
+    SP_CUDA(cudaMemsetAsync(s->umax_dev(), 0, 4 * sizeof(unsigned long long), st));
+    unsigned gv = grid_for(s->fsc, kRedThreads);
+    uint32_t rows = s->fsc / (uint32_t)s->nh;
+    unsigned gm = grid_for((uint64_t)rows * (s->n / 2), kRedThreads);
+    if (gm > (unsigned)kRedBlocks) gm = kRedBlocks;
+    double scale = 1.0 / std::pow((double)s->n, (double)s->dim);
+    for (int c = 0; c < ncomp; ++c) {
+        if (s->fp64) {
+            k_velocity_component<double><<<gv, kRedThreads, 0, st>>>(
+                (const cplx<double>*)state, (cplx<double>*)s->acc, s->n, s->nh, s->dim, s->fsc, c,
+                scale);
+        } else {
+            k_velocity_component<float><<<gv, kRedThreads, 0, st>>>(
+                (const cplx<float>*)state, (cplx<float>*)s->acc, s->n, s->nh, s->dim, s->fsc, c,
+                (float)scale);
+        }
+        SP_CUDA(cudaGetLastError());
+        int r = exec_c2r(s, plan, s->acc, st);
+        if (r) return r;
+        if (s->fp64)
+            k_max_abs_padded<double><<<gm, kRedThreads, 0, st>>>((const double*)s->acc, s->n,
+                                                                 2 * s->nh, rows, s->umax_dev() + c);
+        else
+            k_max_abs_padded<float><<<gm, kRedThreads, 0, st>>>((const float*)s->acc, s->n,
+                                                                2 * s->nh, rows, s->umax_dev() + c);
+        SP_CUDA(cudaGetLastError());
+        s->launches += 2;
+    }
+    unsigned long long bits[4] = {0, 0, 0, 0};
+    SP_CUDA(cudaMemcpyAsync(bits, s->umax_dev(), sizeof(bits), cudaMemcpyDeviceToHost, st));
+    SP_CUDA(cudaStreamSynchronize(st));
+    double sum = 0.0;
+    for (int c = 0; c < ncomp; ++c) {
+        double v;
+        std::memcpy(&v, &bits[c], sizeof(v));
+        if (out_per_comp) out_per_comp[c] = v;
+        sum += v;
+    }
+    if (out_per_comp)
+        for (int c = ncomp; c < 3; ++c) out_per_comp[c] = 0.0;
+    *out_sum = sum;
+    return SP_OK;
+}
+
+int sp_spectrum(sp_solver* s, const void* state, double* out, int nshell, void* stream) {
+    SP_CHECK_BOUND(s);
+    if (!state || !out) return fail(s, SP_ERR_ARG, "sp_spectrum", "null pointer");
+    if (nshell != s->nshell) return fail(s, SP_ERR_ARG, "sp_spectrum", "nshell mismatch");
+    auto st = (cudaStream_t)stream;
+    double norm = std::pow((double)s->n, 2.0 * s->dim);
+    SP_CUDA(cudaMemsetAsync(s->spec_dev(), 0, (size_t)nshell * sizeof(double), st));
+    unsigned g = grid_for(s->fsc, kRedThreads);
+    if (g > (unsigned)kRedBlocks) g = kRedBlocks;
+    size_t smem = (size_t)nshell * sizeof(double);
+    int use_smem = smem <= 48 * 1024 ? 1 : 0;
+    if (!use_smem) smem = 0;
+    if (s->fp64)
+        k_spectrum<double><<<g, kRedThreads, smem, st>>>((const cplx<double>*)state, s->n, s->nh,
+                                                         s->dim, s->fsc, 1.0 / norm, 2.0 / norm,
+                                                         nshell, use_smem, s->spec_dev());
+    else
+        k_spectrum<float><<<g, kRedThreads, smem, st>>>((const cplx<float>*)state, s->n, s->nh,
+                                                        s->dim, s->fsc, 1.0 / norm, 2.0 / norm,
+                                                        nshell, use_smem, s->spec_dev());
+    SP_CUDA(cudaGetLastError());
+    s->launches += 1;
+    SP_CUDA(cudaMemcpyAsync(out, s->spec_dev(), (size_t)nshell * sizeof(double),
+                            cudaMemcpyDeviceToHost, st));
+    SP_CUDA(cudaStreamSynchronize(st));
+    return SP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,265 @@
+"""Device parity: every b200 variant against the fp64 oracle and the reference's own vectors.
+
+Mirrors the reference's cross-backend test (tests/test_backends.py:24-73): same configurations,
+the forcing-amplitude and dt changes mid-run, the exact Taylor-Green decay and device-vs-host
+diagnostics, plus the workload sizes and edge cases.  Tolerances: <= 1e-12 relative (fp64) and
+<= 5e-6 (fp32), max|a - b| / max|b| against the fp64 oracle.
+"""
+
+from __future__ import annotations
+
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle.numpy_oracle import OracleDiagnostics, OracleSolver
+from pyspectral_b200 import BackendUnavailable, Config, initial
+from pyspectral_b200.registry import REGISTRY, get
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = np.load(Path(__file__).parent / "golden" / "reference_vectors.npz")
+TOL = {"float64": 1e-12, "float32": 5e-6}
+VARIANTS = [v for v in REGISTRY if v.gpu]
+
+
+def rel(a: np.ndarray, b: np.ndarray) -> float:
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def _oracle(cfg: Config, **kw) -> OracleSolver:
+    return OracleSolver(cfg.n, cfg.dim, nu=cfg.nu, alpha=cfg.alpha, alpha_kmax=cfg.alpha_kmax,
+                        force_amp=cfg.force_amp, force_klo=cfg.force_klo,
+                        force_khi=cfg.force_khi, dtype=kw.get("dtype", "float64"),
+                        form=cfg.resolved_form())
+
+
+@pytest.mark.parametrize("v", VARIANTS, ids=lambda v: v.name)
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+@pytest.mark.parametrize("dim,form", [(2, "basdevant"), (3, "basdevant"), (3, "rotational")])
+@pytest.mark.parametrize("alpha_kmax", [0.0, 2.0])
+def test_matches_oracle(v, dtype, dim, form, alpha_kmax):
+    n = 32 if dim == 2 else 16
+    cfg = Config(n=n, dim=dim, nu=0.01, alpha=0.5, alpha_kmax=alpha_kmax, force_amp=0.3,
+                 force_klo=1, force_khi=2.5, dtype=dtype, form=form)
+    s = v.make(cfg)
+    ref = _oracle(cfg)
+    ic = (initial.to_spectral(initial.random_2d(n, k0=4), 2) if dim == 2
+          else initial.to_spectral(initial.random_3d(n, k0=2), 3))
+    s.set_state(ic)
+    ref.set_state(ic)
+    s.advance(5, 0.01)
+    ref.advance(5, 0.01)
+    s.set_forcing_amplitude(0.1)
+    ref.set_forcing_amplitude(0.1)
+    s.advance(3, 0.007)
+    ref.advance(3, 0.007)
+    err = rel(s.get_state(), ref.get_state())
+    assert err < TOL[dtype], err
+
+
+@pytest.mark.parametrize("dim,form", [(2, "basdevant"), (3, "basdevant"), (3, "rotational")])
+@pytest.mark.parametrize("akm", [0.0, 2.0])
+def test_matches_reference_vectors(dim, form, akm):
+    """Against the arrays the reference's NumpySolver produced (tests/golden)."""
+    n = 32 if dim == 2 else 16
+    key = f"parity_{dim}d_{form}_akm{int(akm)}"
+    cfg = Config(n=n, dim=dim, nu=0.01, alpha=0.5, alpha_kmax=akm, force_amp=0.3, force_klo=1,
+                 force_khi=2.5, dtype="float64", form=form)
+    s = get("b200").make(cfg)
+    s.set_state(GOLDEN[key + "_ic"])
+    s.advance(5, 0.01)
+    s.set_forcing_amplitude(0.1)
+    s.advance(3, 0.007)
+    assert rel(s.get_state(), GOLDEN[key + "_final"]) < 1e-12
+
+
+@pytest.mark.parametrize("v", VARIANTS, ids=lambda v: v.name)
+def test_tgv2d_exact(v):
+    n, nu = 32, 0.05
+    s = v.make(Config(n=n, dim=2, nu=nu, dtype="float64"))
+    w0 = initial.to_spectral(initial.taylor_green_2d(n), 2)
+    s.set_state(w0)
+    s.advance(20, 0.05)
+    exact = w0 * math.exp(-2 * nu * 1.0)
+    assert rel(s.get_state(), exact) < 1e-13
+
+
+def test_tgv2d_256_fp64_1000_steps():
+    """The plain 2D Taylor-Green workload: 256^2 fp64, nu=1e-2, dt=1e-3, 1000 steps."""
+    n, nu, dt = 256, 1e-2, 1e-3
+    s = get("b200").make(Config(n=n, dim=2, nu=nu, dtype="float64"))
+    w0 = initial.to_spectral(initial.taylor_green_2d(n), 2)
+    s.set_state(w0)
+    s.advance(1000, dt)
+    exact = w0 * math.exp(-2 * nu * s.t)
+    assert rel(s.get_state(), exact) < 1e-12
+    ref = OracleSolver(n, 2, nu=nu)
+    ref.set_state(w0)
+    ref.advance(50, dt)
+    s2 = get("b200").make(Config(n=n, dim=2, nu=nu, dtype="float64"))
+    s2.set_state(w0)
+    s2.advance(50, dt)
+    assert rel(s2.get_state(), ref.get_state()) < 1e-12
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_diagnostics_on_device_match_host(dtype):
+    for dim, n, st in ((3, 16, GOLDEN["diag3d_state"]), (2, 32, GOLDEN["diag2d_state"])):
+        s = get("b200").make(Config(n=n, dim=dim, dtype=dtype))
+        s.set_state(st)
+        h = OracleDiagnostics(n, dim)
+        stq = s.get_state()  # the state as stored (rounded to fp32 if dtype is fp32)
+        tol = 1e-12
+        d = s.diag
+        assert d.energy(s.state_native()) == pytest.approx(h.energy(stq), rel=tol)
+        assert d.enstrophy(s.state_native()) == pytest.approx(h.enstrophy(stq), rel=tol)
+        assert d.palinstrophy(s.state_native()) == pytest.approx(h.palinstrophy(stq), rel=tol)
+        assert d.band_energy(s.state_native(), 1.0, 2.5) == pytest.approx(
+            h.band_energy(stq, 1.0, 2.5), rel=tol)
+        vtol = 1e-12 if dtype == "float64" else 2e-6
+        assert d.max_velocity_sum(s.state_native()) == pytest.approx(
+            h.max_velocity_sum(stq), rel=vtol)
+        np.testing.assert_allclose(d.spectrum(s.state_native())[1], h.spectrum(stq)[1],
+                                   rtol=1e-12, atol=1e-20)
+        if dtype == "float64":
+            vals = GOLDEN[("diag3d" if dim == 3 else "diag2d") + "_values"]
+            got = [d.energy(st), d.enstrophy(st), d.palinstrophy(st), d.band_energy(st, 1, 2.5),
+                   d.max_velocity_sum(st)]
+            np.testing.assert_allclose(got, vals, rtol=1e-12)
+
+
+def test_diagnostics_are_deterministic():
+    s = get("b200").make(Config(n=64, dim=2, dtype="float32"))
+    s.set_state(initial.random_phase_2d(64, k0=8, seed=1))
+    a = [s.diag.all(s.state_native(), 1, 3) for _ in range(3)]
+    assert a[0] == a[1] == a[2]
+
+
+def test_tgv3d_initial_diagnostics_on_device():
+    s = get("b200").make(Config(n=16, dim=3, dtype="float64"))
+    u = initial.to_spectral(initial.taylor_green_3d(16), 3)
+    s.set_state(u)
+    assert s.diag.energy(s.state_native()) == pytest.approx(0.125, rel=1e-13)
+    assert s.diag.enstrophy(s.state_native()) == pytest.approx(0.375, rel=1e-13)
+    assert s.diag.spectrum(s.state_native())[1].sum() == pytest.approx(0.125, rel=1e-13)
+
+
+def test_graph_and_plain_launches_are_bitwise_identical():
+    cfg = Config(n=64, dim=2, nu=1e-3, alpha=0.1, alpha_kmax=2, force_amp=0.2, force_klo=3,
+                 force_khi=5, dtype="float32")
+    ic = initial.random_phase_2d(64, k0=8, seed=2)
+    out = []
+    for name in ("b200/fused-inplace", "b200/fused-inplace-graph", "b200/fused-inplace-lean"):
+        s = get(name).make(cfg)
+        s.set_state(ic)
+        for k in range(12):  # dt and amplitude change while the same graph is replayed
+            s.set_forcing_amplitude(0.2 + 0.01 * k)
+            s.step(1e-3 * (1 + 0.1 * k))
+        out.append(s.get_state())
+    assert np.array_equal(out[0], out[1])
+    assert np.array_equal(out[0], out[2])
+
+
+def test_dealiased_modes_stay_zero_and_state_is_hermitian():
+    n = 48
+    s = get("b200").make(Config(n=n, dim=2, nu=1e-3, dtype="float64"))
+    s.set_state(initial.random_phase_2d(n, k0=6, seed=5))
+    s.advance(10, 2e-3)
+    st = s.get_state()
+    from pyspectral_b200.grid import dealias_mask
+
+    assert np.all(st[~dealias_mask(n, 2)] == 0)
+    col = st[:, 0]
+    np.testing.assert_allclose(col[1:n // 2], np.conj(col[n - 1:n // 2:-1]),
+                               atol=1e-12 * np.abs(st).max())
+
+
+@pytest.mark.parametrize("n", [8, 10, 34])
+def test_small_and_non_power_of_two_grids(n):
+    for dim, form in ((2, "basdevant"), (3, "rotational")):
+        cfg = Config(n=n, dim=dim, nu=0.02, alpha=0.3, dtype="float64", form=form)
+        s = get("b200").make(cfg)
+        ref = _oracle(cfg)
+        ic = (initial.to_spectral(initial.random_2d(n, k0=2), 2) if dim == 2
+              else initial.to_spectral(initial.random_3d(n, k0=1.5), 3))
+        s.set_state(ic)
+        ref.set_state(ic)
+        s.advance(4, 0.01)
+        ref.advance(4, 0.01)
+        assert rel(s.get_state(), ref.get_state()) < 1e-12
+
+
+def test_forcing_switch_off_and_on_and_set_state_resets():
+    cfg = Config(n=32, dim=2, nu=0.0, force_amp=1.0, force_klo=1, force_khi=1.5,
+                 dtype="float64")
+    s = get("b200").make(cfg)
+    w0 = initial.to_spectral(initial.taylor_green_2d(32), 2)
+    s.set_state(w0)
+    s.advance(10, 0.01)
+    np.testing.assert_allclose(s.get_state(), w0 * math.exp(0.1), rtol=1e-12, atol=1e-9)
+    s.set_forcing_amplitude(0.0)
+    s.advance(5, 0.01)
+    np.testing.assert_allclose(s.get_state(), w0 * math.exp(0.1), rtol=1e-12, atol=1e-9)
+    s.set_state(w0)
+    s.set_forcing_amplitude(-2.0)
+    s.advance(5, 0.01)
+    np.testing.assert_allclose(s.get_state(), w0 * math.exp(-0.1), rtol=1e-12, atol=1e-9)
+
+
+def test_errors_are_reported():
+    with pytest.raises(BackendUnavailable):
+        get("b200").make(Config(n=16, dim=2, form="advective"))
+    with pytest.raises(BackendUnavailable):
+        get("b200").make(Config(n=16, dim=2, dealias="phase-shift"))
+    s = get("b200").make(Config(n=16, dim=2))
+    with pytest.raises(ValueError):
+        s.set_state(np.zeros((16, 16), complex))
+
+
+def test_workload_8192_fp32_properties():
+    """The 8192^2 fp32 decaying-turbulence workload: size-independent checks at full size.
+
+    Energy must follow dE/dt = -2 nu Z (no forcing), the CFL bound must match a direct
+    per-component maximum, and the run must be bit-reproducible."""
+    n, nu = 8192, 2e-6
+    cfg = Config(n=n, dim=2, nu=nu, dtype="float32")
+    w0 = initial.random_phase_2d(n, k0=12, seed=0, energy=0.5)
+    s = get("b200").make(cfg)
+    s.set_state(w0)
+    d = s.diag
+    e0 = d.energy(s.state_native())
+    assert e0 == pytest.approx(0.5, rel=1e-6)
+    umax, per = d.max_velocity(s.state_native())
+    dt = 0.5 * (2 * math.pi / n) / umax
+    es, zs = [], []
+    for _ in range(3):
+        es.append(d.energy(s.state_native()))
+        zs.append(d.enstrophy(s.state_native()))
+        s.step(dt)
+    dedt = (es[2] - es[0]) / (2 * dt)
+    assert dedt < 0
+    assert abs(dedt + 2 * nu * zs[1]) < 2e-2 * abs(2 * nu * zs[1])
+    first = s.get_state()
+    s2 = get("b200").make(cfg)
+    s2.set_state(w0)
+    for _ in range(3):
+        s2.step(dt)
+    assert np.array_equal(first, s2.get_state())
+
+
+def test_workload_8192_fp32_matches_oracle_one_step():
+    """One CFL step of the 8192^2 fp32 workload against the fp64 oracle."""
+    n = 8192
+    cfg = Config(n=n, dim=2, nu=2e-6, dtype="float32")
+    w0 = initial.random_phase_2d(n, k0=12, seed=0, energy=0.5)
+    s = get("b200").make(cfg)
+    s.set_state(w0)
+    dt = 1e-4
+    s.step(dt)
+    ref = OracleSolver(n, 2, nu=2e-6)
+    ref.set_state(w0)
+    ref.step(dt)
+    assert rel(s.get_state(), ref.get_state()) < 1e-5
