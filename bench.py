@@ -42,6 +42,9 @@ WORKLOADS = {
     # the decaying-turbulence headline: 8192^2 fp32, CFL 0.5, 200 steps in the full run
     "decay2d-8192-fp32": dict(n=8192, dim=2, dtype="float32", nu=2e-6, form="basdevant",
                               ic="random_phase", k0=12.0, seed=0, energy=0.5, cfl=0.5),
+    # the same flow on 4096^2 (profiling captures that must stay small)
+    "decay2d-4096-fp32": dict(n=4096, dim=2, dtype="float32", nu=8e-6, form="basdevant",
+                              ic="random_phase", k0=12.0, seed=0, energy=0.5, cfl=0.5),
     # plain 2D Taylor-Green: 256^2 fp64, nu=1e-2, fixed dt=1e-3
     "tgv2d-256-fp64": dict(n=256, dim=2, dtype="float64", nu=1e-2, form="basdevant",
                            ic="tgv2d", dt=1e-3),
@@ -322,6 +325,22 @@ def ours(args, w: dict) -> int:
     del s2, out
     torch.cuda.empty_cache()
 
+    # ---- error of one step against the fp64 engine (itself pinned to the fp64 oracle)
+    rel_err = None
+    if w["dtype"] == "float32":
+        a = make_solver(args.variant, cfg)
+        b = make_solver(args.variant, cfg.with_(dtype="float64"))
+        a.set_state(ic)
+        b.set_state(ic)
+        h = w.get("dt") or min(0.05, w["cfl"] * (2 * math.pi / w["n"])
+                               / b.diag.max_velocity_sum(b.state_native()))
+        a.step(h)
+        b.step(h)
+        ra, rb = a.get_state(), b.get_state()
+        rel_err = float(abs(ra - rb).max() / abs(rb).max())
+        del a, b, ra, rb
+        torch.cuda.empty_cache()
+
     # ---- per-phase device times (state garbage afterwards: nothing reads it)
     def fft_stage() -> None:
         s.run_phase(0)
@@ -378,6 +397,7 @@ def ours(args, w: dict) -> int:
                 "h2d_bytes_per_step": state_bytes / args.steps,
                 "d2h_bytes_per_step": (state_bytes + cfl_reads) / args.steps,
                 "what": "set_state(host) + K steps + get_state(host), wall clock"},
+        "rel_err_one_step_vs_fp64": rel_err,
         "gpu_launches": launches,
         "clocks": clk,
     }

@@ -192,3 +192,58 @@ def test_run_steps_is_cfl_every_10():
     assert len(dts) == 25
     assert len(set(dts[:10])) == 1 and len(set(dts[10:20])) == 1
     assert math.isclose(sum(dts), s.t)
+
+
+# ----------------------------------------------------------------------------- pyspectral plugin
+def _pyspectral_importable() -> bool:
+    import importlib.util
+    import sys
+
+    src = "/root/reference/src"
+    if importlib.util.find_spec("pyspectral") is None and Path(src).exists():
+        sys.path.append(src)
+    return importlib.util.find_spec("pyspectral") is not None
+
+
+@pytest.mark.skipif(not _pyspectral_importable(), reason="pyspectral not importable here")
+def test_plugin_registers_into_pyspectral_registry(capsys):
+    from pyspectral.backends import REGISTRY as REF, BackendUnavailable as RefUnavailable
+    from pyspectral.backends import get as ref_get
+    from pyspectral.backends.base import SpectralSolver as RefSolver
+    from pyspectral.cli import main as ref_cli
+    from pyspectral.config import Config as RefConfig
+
+    from pyspectral_b200.pyspectral_plugin import register
+
+    before = len(REF)
+    added = register()
+    register()  # idempotent
+    try:
+        assert len(REF) == before + 3 == before + len(added)
+        v = ref_get("b200")
+        assert v.name == "b200/fused-inplace-graph"
+        cls = v.load()
+        assert issubclass(cls, RefSolver)
+        ok, why = v.available()
+        import torch
+
+        if not torch.cuda.is_available():
+            assert not ok and "CUDA" in why
+            with pytest.raises(RefUnavailable):
+                v.make(RefConfig(n=16))
+        assert ref_cli(["list"]) == 0
+        assert "b200/fused-inplace-graph" in capsys.readouterr().out
+    finally:
+        del REF[before:]
+
+
+@pytest.mark.skipif(not _pyspectral_importable(), reason="pyspectral not importable here")
+def test_plugin_class_raises_pyspectral_unavailable():
+    from pyspectral.backends.base import BackendUnavailable as RefUnavailable
+    from pyspectral.config import Config as RefConfig
+
+    from pyspectral_b200.pyspectral_plugin import _plugin_class
+
+    cls = _plugin_class("B200Solver")
+    with pytest.raises(RefUnavailable):
+        cls(RefConfig(n=16, dim=2, form="advective"))
