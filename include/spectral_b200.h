@@ -153,8 +153,30 @@ int64_t sp_kernel_launches(const sp_solver* s);
 /* Message of the last failure on this handle (never NULL). */
 const char* sp_last_error(const sp_solver* s);
 
-/* Message of the last sp_create failure in this thread (never NULL). */
+/* Message of the last sp_create (or sp_spectrum_noalloc) failure in this thread (never NULL). */
 const char* sp_create_error(void);
+
+/* Largest number of spectrum shells sp_spectrum_noalloc accepts: its accumulators are a fixed
+ * file-scope device array of this many doubles (128 KiB).  2D grids up to n = 23168 fit, and
+ * every 3D grid the engine indexes with 32 bits (n <= 1290). */
+#define SP_NOALLOC_MAX_SHELLS 16384
+
+/* Shell-summed energy spectrum E(k), k = 0..nshell-1, of a device state (u0 layout, fp32 or
+ * fp64 complex) written to the host array `out` — without an engine handle and without
+ * allocating any device memory.  No counterpart in the reference: it is for callers that must
+ * not allocate device memory (a program whose own pool allocator owns the GPU's memory, or a
+ * loop that may not take cudaMalloc's implicit synchronisation) yet need the spectrum of a state
+ * they hold.  Same values as sp_spectrum.
+ *   - Scratch: a file-scope __device__ array of SP_NOALLOC_MAX_SHELLS doubles, held by every GPU
+ *     that loads the library until the process exits.  Each call clears the shells it uses.
+ *   - The first call on a device looks the array's device address up (cudaGetSymbolAddress, with
+ *     that device current) and caches it; make that first call before any stream capture.
+ *   - Calls share the array: two calls whose work overlaps on the GPU race and give wrong
+ *     results; order them on one stream.
+ *   - Returns SP_ERR_ARG (message in sp_create_error()) when nshell does not match n and dim, or
+ *     exceeds SP_NOALLOC_MAX_SHELLS; synchronises `stream`. */
+int sp_spectrum_noalloc(const void* state, int n, int dim, int fp64, double* out, int nshell,
+                        void* stream);
 
 #ifdef __cplusplus
 }

@@ -47,6 +47,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_kernel_launches": (ctypes.c_int64, [_vp]),
     "sp_last_error": (ctypes.c_char_p, [_vp]),
     "sp_create_error": (ctypes.c_char_p, []),
+    "sp_spectrum_noalloc": (_i, [_vp, _i, _i, _i, _dp, _i, _vp]),
 }
 
 _LIB: ctypes.CDLL | None = None

@@ -51,6 +51,11 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 }  // namespace
 
+namespace sp {
+// Thread-local message behind sp_create_error(); also set by sp_spectrum_noalloc.
+void set_thread_error(const char* why) { g_create_error = why; }
+}  // namespace sp
+
 struct sp_solver {
     // grid
     int n = 0, dim = 0, form = 0, fp64 = 0, fft_mode = 0;
