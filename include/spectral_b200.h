@@ -51,8 +51,15 @@ enum sp_form { SP_FORM_BASDEVANT = 0, SP_FORM_ROTATIONAL = 1 };
 /* How the FFTs of a stage are executed.
  *   SP_FFT_CUFFT       batched in-place cuFFT plans (cupy_cuda.py:100-112, variant fused-inplace)
  *   SP_FFT_CUFFT_LEAN  single-field plans looped over the batch (cupy_cuda.py:114-128,
- *                      variant fused-inplace-lean: cuFFT workspace of one field)            */
-enum sp_fft_mode { SP_FFT_CUFFT = 0, SP_FFT_CUFFT_LEAN = 1 };
+ *                      variant fused-inplace-lean: cuFFT workspace of one field)
+ *   SP_FFT_FUSED       2D only: hand-written transforms fused with the pointwise phases, two
+ *                      HBM round trips per RK stage (a row pass: inverse row FFT, products,
+ *                      forward row FFT; a column pass: forward column FFT, Lawson update,
+ *                      inverse column FFT) over the 2/3-dealiased columns only.  n a power of
+ *                      two, 16..8192 (fp32) or 16..4096 (fp64); no cuFFT.  The state is kept
+ *                      transposed internally; u0 is refreshed by sp_sync_state (and by the
+ *                      diagnostics entry points when given u0). */
+enum sp_fft_mode { SP_FFT_CUFFT = 0, SP_FFT_CUFFT_LEAN = 1, SP_FFT_FUSED = 2 };
 
 /* Indices of the array filled by sp_query_sizes(). */
 enum sp_size_index {
@@ -118,6 +125,12 @@ int sp_prepare(sp_solver* s, void* stream);
  * amplitude (no re-capture per (dt, amp) as at cupy_cuda.py:181-195). */
 int sp_step(sp_solver* s, double dt, void* stream);
 
+/* Make u0 (the NumPy-layout state) current.  In SP_FFT_FUSED mode the step advances a
+ * transposed copy of the state and u0 is written back here, once per change; in the cuFFT
+ * modes u0 is always current and this does nothing.  Call before reading u0 directly
+ * (state_native(), base.py:65-67). */
+int sp_sync_state(sp_solver* s, void* stream);
+
 /* 1 = replay each step from a CUDA graph (variant fused-inplace-graph), 0 = plain launches. */
 int sp_set_graph(sp_solver* s, int enable);
 
@@ -130,6 +143,8 @@ int sp_diagnostics(sp_solver* s, const void* state, double band_klo, double band
 /* sum_i max|u_i| in physical space of a state array (Diagnostics.max_velocity_sum,
  * src/pyspectral/diagnostics.py:99-109); out_per_comp (host, 3 doubles, may be NULL) receives
  * each component's max.  Uses the RK accumulator as scratch (it is dead between steps).
+ * In SP_FFT_FUSED mode only `state == u0` is accepted (SP_ERR_UNSUPPORTED otherwise): the
+ * bound comes from one inverse row pass over the stage-0 inputs already in the work array.
  * Synchronises `stream`. */
 int sp_max_velocity(sp_solver* s, const void* state, double* out_sum, double* out_per_comp,
                     void* stream);
@@ -141,6 +156,7 @@ int sp_spectrum(sp_solver* s, const void* state, double* out, int nshell, void* 
 /* Run one phase of one stage by itself (for per-phase timing and profiling):
  * phase 0 = batched inverse FFT, 1 = physical-space kernel, 2 = batched forward FFT,
  * 3 = spectral kernel of RK stage `stage` (0..3) using the parameters of the last step.
+ * In SP_FFT_FUSED mode phase 0 is the row pass, 3 the column pass, 1 and 2 do nothing.
  * Phases 0+2 back to back are the standalone "FFT ceiling" of one stage
  * (src/pyspectral/benchmark.py:145-214). */
 int sp_run_phase(sp_solver* s, int phase, int stage, void* stream);

@@ -20,7 +20,7 @@ STATUS_NAMES = {0: "SP_OK", -1: "SP_ERR_ARG", -2: "SP_ERR_CUDA", -3: "SP_ERR_CUF
                 -4: "SP_ERR_STATE", -5: "SP_ERR_UNSUPPORTED"}
 # enum sp_form / sp_fft_mode
 FORM_CODES = {"basdevant": 0, "rotational": 1}
-FFT_CUFFT, FFT_CUFFT_LEAN = 0, 1
+FFT_CUFFT, FFT_CUFFT_LEAN, FFT_FUSED = 0, 1, 2
 # enum sp_size_index
 SZ_MODES, SZ_NCOMP, SZ_NWORK, SZ_NINV, SZ_NFWD = 0, 1, 2, 3, 4
 SZ_STATE_BYTES, SZ_WORK_BYTES, SZ_AUX_BYTES, SZ_FFTWS_BYTES, SZ_NSHELL, SZ_COUNT = 5, 6, 7, 8, 9, 10
@@ -39,6 +39,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_set_forcing_amplitude": (_i, [_vp, _d]),
     "sp_prepare": (_i, [_vp, _vp]),
     "sp_step": (_i, [_vp, _d, _vp]),
+    "sp_sync_state": (_i, [_vp, _vp]),
     "sp_set_graph": (_i, [_vp, _i]),
     "sp_diagnostics": (_i, [_vp, _vp, _d, _d, _dp, _vp]),
     "sp_max_velocity": (_i, [_vp, _vp, _dp, _dp, _vp]),

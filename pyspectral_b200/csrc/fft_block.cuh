@@ -1,0 +1,335 @@
+// Block-level complex FFT of length N (power of two, 16..8192) in shared memory and registers.
+//
+// A sub-block of T = N/16 threads transforms one length-N sequence; every thread keeps 16
+// elements in registers across all passes.  The transform is a Stockham (self-sorting) radix
+// sequence: radix-16 passes plus at most one radix-2/4/8 pass, so 8192 = 16*16*16*2 takes four
+// passes with three shared-memory exchanges.  Pass p with radix R and stride S reads element m
+// of group j at j + m*N/R, multiplies it by w_{S R}^{(j mod S) m}, does an R-point DFT and
+// writes output m to (j div S) S R + (j mod S) + m S.  The last pass of a transform therefore
+// leaves output j + m*N/R in the same thread and register that the first pass of a transform
+// with the same radix reads its input from: an inverse transform ending with radix R feeds a
+// forward transform starting with radix R without any exchange (and vice versa).
+//
+// Elements are either one complex sequence (cplx<T>) or two sequences sharing the transform
+// (Pair<T>).  Twiddles come from a table tw[i] = exp(+2 pi i i/N) (fp64 on the host, rounded
+// to T); the forward transform conjugates them.  DIR = +1: inverse (e^{+}), DIR = -1: forward.
+#pragma once
+
+#include "common.cuh"
+
+namespace sp {
+
+template <typename T>
+struct Pair {
+    cplx<T> a, b;
+};
+
+// ---------------------------------------------------------------------------- element algebra
+template <typename C>
+__device__ __forceinline__ C cmul(C x, C w) {
+    C r;
+    r.x = fma(x.x, w.x, -x.y * w.y);
+    r.y = fma(x.x, w.y, x.y * w.x);
+    return r;
+}
+template <typename C>
+__device__ __forceinline__ C csub(C x, C y) {
+    C r;
+    r.x = x.x - y.x;
+    r.y = x.y - y.y;
+    return r;
+}
+// x * (dir * i)
+template <int DIR, typename C>
+__device__ __forceinline__ C cmul_i(C x) {
+    C r;
+    if (DIR > 0) { r.x = -x.y; r.y = x.x; }
+    else { r.x = x.y; r.y = -x.x; }
+    return r;
+}
+
+__device__ __forceinline__ float2 eadd(float2 x, float2 y) { return add(x, y); }
+__device__ __forceinline__ double2 eadd(double2 x, double2 y) { return add(x, y); }
+__device__ __forceinline__ float2 esub(float2 x, float2 y) { return csub(x, y); }
+__device__ __forceinline__ double2 esub(double2 x, double2 y) { return csub(x, y); }
+__device__ __forceinline__ float2 emul(float2 x, float2 w) { return cmul(x, w); }
+__device__ __forceinline__ double2 emul(double2 x, double2 w) { return cmul(x, w); }
+template <int DIR> __device__ __forceinline__ float2 emul_i(float2 x) { return cmul_i<DIR>(x); }
+template <int DIR> __device__ __forceinline__ double2 emul_i(double2 x) { return cmul_i<DIR>(x); }
+__device__ __forceinline__ float2 escale(float2 x, float s) { return scl(s, x); }
+__device__ __forceinline__ double2 escale(double2 x, double s) { return scl(s, x); }
+
+template <typename T>
+__device__ __forceinline__ Pair<T> eadd(Pair<T> x, Pair<T> y) { return {add(x.a, y.a), add(x.b, y.b)}; }
+template <typename T>
+__device__ __forceinline__ Pair<T> esub(Pair<T> x, Pair<T> y) { return {csub(x.a, y.a), csub(x.b, y.b)}; }
+template <typename T>
+__device__ __forceinline__ Pair<T> emul(Pair<T> x, cplx<T> w) { return {cmul(x.a, w), cmul(x.b, w)}; }
+template <int DIR, typename T>
+__device__ __forceinline__ Pair<T> emul_i(Pair<T> x) { return {cmul_i<DIR>(x.a), cmul_i<DIR>(x.b)}; }
+template <typename T>
+__device__ __forceinline__ Pair<T> escale(Pair<T> x, T s) { return {scl(s, x.a), scl(s, x.b)}; }
+
+template <typename E> struct ElemReal;
+template <> struct ElemReal<float2> { using type = float; };
+template <> struct ElemReal<double2> { using type = double; };
+template <> struct ElemReal<Pair<float>> { using type = float; };
+template <> struct ElemReal<Pair<double>> { using type = double; };
+
+// ---------------------------------------------------------------------------- small DFTs
+// X_k = sum_n x_n w^{n k}, w = exp(DIR * 2 pi i / R), in place, natural order in and out.
+template <int DIR, typename E>
+__device__ __forceinline__ void dft2(E* x) {
+    E t = esub(x[0], x[1]);
+    x[0] = eadd(x[0], x[1]);
+    x[1] = t;
+}
+
+template <int DIR, typename E>
+__device__ __forceinline__ void dft4(E& x0, E& x1, E& x2, E& x3) {
+    E a = eadd(x0, x2), b = esub(x0, x2), c = eadd(x1, x3), d = emul_i<DIR>(esub(x1, x3));
+    x0 = eadd(a, c);
+    x2 = esub(a, c);
+    x1 = eadd(b, d);
+    x3 = esub(b, d);
+}
+
+template <int DIR, typename E>
+__device__ __forceinline__ void dft4(E* x) { dft4<DIR>(x[0], x[1], x[2], x[3]); }
+
+// multiply by exp(DIR * 2 pi i * q / 16) for q in 0..15 given as a compile-time constant
+template <int DIR, int Q, typename E>
+__device__ __forceinline__ E rot16(E x) {
+    using R = typename ElemReal<E>::type;
+    constexpr int q = Q & 15;
+    const R c1 = (R)0.92387953251128675613, s1 = (R)0.38268343236508977173;  // cos, sin(pi/8)
+    const R h = (R)0.70710678118654752440;                                     // sqrt(2)/2
+    if (q == 0) return x;
+    if (q == 4) return emul_i<DIR>(x);
+    if (q == 8) return escale(x, (R)-1);
+    if (q == 12) return emul_i<-DIR>(x);
+    // generic: exp(i theta) with theta = DIR * q * pi / 8
+    R cs, sn;
+    switch (q) {
+        case 1: cs = c1; sn = s1; break;
+        case 2: cs = h; sn = h; break;
+        case 3: cs = s1; sn = c1; break;
+        case 5: cs = -s1; sn = c1; break;
+        case 6: cs = -h; sn = h; break;
+        case 7: cs = -c1; sn = s1; break;
+        case 9: cs = -c1; sn = -s1; break;
+        case 10: cs = -h; sn = -h; break;
+        case 11: cs = -s1; sn = -c1; break;
+        case 13: cs = s1; sn = -c1; break;
+        case 14: cs = h; sn = -h; break;
+        default: cs = c1; sn = -s1; break;  // 15
+    }
+    cplx<R> w = mk<R>(cs, DIR > 0 ? sn : -sn);
+    return emul(x, w);
+}
+
+template <int DIR, typename E>
+__device__ __forceinline__ void dft8(E* x) {
+    // even/odd split: X_k = E_k + w8^k O_k, X_{k+4} = E_k - w8^k O_k
+    E e[4] = {x[0], x[2], x[4], x[6]}, o[4] = {x[1], x[3], x[5], x[7]};
+    dft4<DIR>(e);
+    dft4<DIR>(o);
+    o[1] = rot16<DIR, 2>(o[1]);
+    o[2] = rot16<DIR, 4>(o[2]);
+    o[3] = rot16<DIR, 6>(o[3]);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        x[k] = eadd(e[k], o[k]);
+        x[k + 4] = esub(e[k], o[k]);
+    }
+}
+
+template <int DIR, typename E>
+__device__ __forceinline__ void dft16(E* x) {
+    // n = 4 n1 + n2, k = k1 + 4 k2: inner DFT4 over n1, twiddle w16^{n2 k1}, outer DFT4 over n2
+    E y[16];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+        E a = x[n2], b = x[4 + n2], c = x[8 + n2], d = x[12 + n2];
+        dft4<DIR>(a, b, c, d);  // k1 = 0..3
+        y[n2 * 4 + 0] = a;
+        y[n2 * 4 + 1] = b;
+        y[n2 * 4 + 2] = c;
+        y[n2 * 4 + 3] = d;
+    }
+    y[1 * 4 + 1] = rot16<DIR, 1>(y[1 * 4 + 1]);
+    y[1 * 4 + 2] = rot16<DIR, 2>(y[1 * 4 + 2]);
+    y[1 * 4 + 3] = rot16<DIR, 3>(y[1 * 4 + 3]);
+    y[2 * 4 + 1] = rot16<DIR, 2>(y[2 * 4 + 1]);
+    y[2 * 4 + 2] = rot16<DIR, 4>(y[2 * 4 + 2]);
+    y[2 * 4 + 3] = rot16<DIR, 6>(y[2 * 4 + 3]);
+    y[3 * 4 + 1] = rot16<DIR, 3>(y[3 * 4 + 1]);
+    y[3 * 4 + 2] = rot16<DIR, 6>(y[3 * 4 + 2]);
+    y[3 * 4 + 3] = rot16<DIR, 9>(y[3 * 4 + 3]);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        E a = y[0 * 4 + k1], b = y[1 * 4 + k1], c = y[2 * 4 + k1], d = y[3 * 4 + k1];
+        dft4<DIR>(a, b, c, d);  // k2 = 0..3
+        x[k1 + 0] = a;
+        x[k1 + 4] = b;
+        x[k1 + 8] = c;
+        x[k1 + 12] = d;
+    }
+}
+
+template <int R, int DIR, typename E>
+__device__ __forceinline__ void dftR(E* x) {
+    if constexpr (R == 2) dft2<DIR>(x);
+    else if constexpr (R == 4) dft4<DIR>(x);
+    else if constexpr (R == 8) dft8<DIR>(x);
+    else dft16<DIR>(x);
+}
+
+// ---------------------------------------------------------------------------- pass plan
+constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
+
+template <int N>
+struct FftPlan {
+    static constexpr int LOG = ilog2(N);
+    static constexpr int A = LOG / 4;                 // radix-16 passes
+    static constexpr int R0 = 1 << (LOG % 4);         // remainder radix (1 = none)
+    static constexpr int NP = A + (R0 > 1 ? 1 : 0);   // passes per transform
+    static constexpr int T = N / 16;                  // threads per sequence
+    static constexpr int SMEM = N + N / 16;           // padded elements per sequence
+    static_assert((1 << LOG) == N && N >= 16 && N <= 8192, "N must be a power of two, 16..8192");
+    // inverse order: 16, 16, ..., R0 ; forward order: R0, 16, ..., 16
+    static constexpr int radix(bool inv, int p) {
+        return inv ? (p < A ? 16 : R0) : ((R0 > 1 && p == 0) ? R0 : 16);
+    }
+    static constexpr int stride(bool inv, int p) {  // product of the previous radices
+        int s = 1;
+        for (int q = 0; q < p; ++q) s *= radix(inv, q);
+        return s;
+    }
+};
+
+// shared-memory index with one pad element every 16 (conflict-free strided access)
+__device__ __forceinline__ int spad(int e) { return e + (e >> 4); }
+
+// position of register v[g*R + m] for a pass of radix R: input pattern j + m N/R
+template <int N, int R>
+__device__ __forceinline__ int in_pos(int t, int g, int m) {
+    return t + (N / 16) * g + m * (N / R);
+}
+
+template <int DIR, typename C>
+__device__ __forceinline__ C tw_load(const C* __restrict__ tw, int idx) {
+    C w = __ldg(tw + idx);
+    if (DIR < 0) w.y = -w.y;
+    return w;
+}
+
+// Twiddles w^m, m = 1..R-1, of one group: three table loads (w, w^4, w^8) and at most three
+// dependent complex products for the others, instead of R-1 scattered table loads.
+template <int R, int DIR, typename C>
+__device__ __forceinline__ void group_twiddles(C (&w)[16], const C* __restrict__ tw, int base) {
+    w[1] = tw_load<DIR>(tw, base);
+    if constexpr (R >= 4) {
+        w[2] = cmul(w[1], w[1]);
+        w[3] = cmul(w[2], w[1]);
+    }
+    if constexpr (R >= 8) {
+        w[4] = tw_load<DIR>(tw, 4 * base);
+        w[5] = cmul(w[4], w[1]);
+        w[6] = cmul(w[4], w[2]);
+        w[7] = cmul(w[4], w[3]);
+    }
+    if constexpr (R >= 16) {
+        w[8] = tw_load<DIR>(tw, 8 * base);
+        w[9] = cmul(w[8], w[1]);
+        w[10] = cmul(w[8], w[2]);
+        w[11] = cmul(w[8], w[3]);
+        w[12] = cmul(w[8], w[4]);
+        w[13] = cmul(w[12], w[1]);
+        w[14] = cmul(w[12], w[2]);
+        w[15] = cmul(w[12], w[3]);
+    }
+}
+
+template <int N, int R, int S, int DIR, typename E, typename C>
+__device__ __forceinline__ void pass_compute(E (&v)[16], int t, const C* __restrict__ tw) {
+    constexpr int G = 16 / R;
+    constexpr int T = N / 16;
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        if constexpr (S > 1) {
+            // w_{S R}^{js m} = w_N^{js m N/(S R)}; the index of w^8 stays below N
+            const int js = (t + T * g) & (S - 1);
+            C w[16];
+            group_twiddles<R, DIR>(w, tw, js * (N / (S * R)));
+#pragma unroll
+            for (int m = 1; m < R; ++m) v[g * R + m] = emul(v[g * R + m], w[m]);
+        }
+        dftR<R, DIR>(v + g * R);
+    }
+}
+
+template <int N, int R, typename E>
+__device__ __forceinline__ void pass_load(E (&v)[16], const E* sm, int t) {
+    constexpr int G = 16 / R;
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int m = 0; m < R; ++m) v[g * R + m] = sm[spad(in_pos<N, R>(t, g, m))];
+}
+
+template <int N, int R, int S, typename E>
+__device__ __forceinline__ void pass_store(const E (&v)[16], E* sm, int t) {
+    constexpr int G = 16 / R;
+    constexpr int T = N / 16;
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        const int j = t + T * g;
+        const int base = (j / S) * S * R + (j & (S - 1));
+#pragma unroll
+        for (int m = 0; m < R; ++m) sm[spad(base + m * S)] = v[g * R + m];
+    }
+}
+
+// Full transform.  On entry v holds the input in the pattern of pass 0 (in_pos with radix
+// radix(INV, 0)); on exit v holds the output at in_pos with the last pass's radix.  `sm` is this
+// sequence's padded shared buffer; every thread of the CTA must call (barriers inside).
+template <int N, bool INV, typename E, typename C>
+__device__ __forceinline__ void block_fft(E (&v)[16], E* sm, int t, const C* __restrict__ tw) {
+    using P = FftPlan<N>;
+    constexpr int DIR = INV ? 1 : -1;
+    constexpr int R0 = P::radix(INV, 0), S0 = P::stride(INV, 0);
+    pass_compute<N, R0, S0, DIR>(v, t, tw);
+    if constexpr (P::NP > 1) {
+        constexpr int R1 = P::radix(INV, 1), S1 = P::stride(INV, 1);
+        pass_store<N, R0, S0>(v, sm, t);
+        __syncthreads();
+        pass_load<N, R1>(v, sm, t);
+        __syncthreads();
+        pass_compute<N, R1, S1, DIR>(v, t, tw);
+        if constexpr (P::NP > 2) {
+            constexpr int R2 = P::radix(INV, 2), S2 = P::stride(INV, 2);
+            pass_store<N, R1, S1>(v, sm, t);
+            __syncthreads();
+            pass_load<N, R2>(v, sm, t);
+            __syncthreads();
+            pass_compute<N, R2, S2, DIR>(v, t, tw);
+            if constexpr (P::NP > 3) {
+                constexpr int R3 = P::radix(INV, 3), S3 = P::stride(INV, 3);
+                pass_store<N, R2, S2>(v, sm, t);
+                __syncthreads();
+                pass_load<N, R3>(v, sm, t);
+                __syncthreads();
+                pass_compute<N, R3, S3, DIR>(v, t, tw);
+            }
+        }
+    }
+}
+
+// radix of the last pass (output pattern) and of the first pass (input pattern)
+template <int N, bool INV>
+constexpr int first_radix() { return FftPlan<N>::radix(INV, 0); }
+template <int N, bool INV>
+constexpr int last_radix() { return FftPlan<N>::radix(INV, FftPlan<N>::NP - 1); }
+
+}  // namespace sp

@@ -1,0 +1,173 @@
+// Launchers of the fused 2D engine: runtime grid size -> compile-time kernel instantiation.
+#include "fused2d.h"
+#include "fused2d.cuh"
+
+namespace sp {
+namespace fused {
+
+namespace {
+
+template <typename T, int N>
+cudaError_t attrs() {
+    using F = Fused2D<N>;
+    const int row_smem = (int)RowPairs<N>::smem_bytes(sizeof(Pair<T>));
+    const int col_smem = (int)F::template smem_bytes<Pair<T>>();
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_row_pass<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  row_smem)))
+        return e;
+    if ((e = cudaFuncSetAttribute(k_row_max<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  row_smem)))
+        return e;
+    if ((e = cudaFuncSetAttribute(k_col_pass<T, N, -1>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
+        return e;
+    if ((e = cudaFuncSetAttribute(k_col_pass<T, N, 0>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
+        return e;
+    if ((e = cudaFuncSetAttribute(k_col_pass<T, N, 1>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
+        return e;
+    if ((e = cudaFuncSetAttribute(k_col_pass<T, N, 2>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
+        return e;
+    return cudaFuncSetAttribute(k_col_pass<T, N, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                col_smem);
+}
+
+template <typename T, int N>
+cudaError_t row(void* X, int kc, const void* tw, cudaStream_t st) {
+    using F = RowPairs<N>;
+    k_row_pass<T, N><<<(N / 2) / F::B, F::THREADS, F::smem_bytes(sizeof(Pair<T>)), st>>>(
+        (Pair<T>*)X, kc, (const cplx<T>*)tw);
+    return cudaGetLastError();
+}
+
+template <typename T, int N>
+cudaError_t rmax(const void* X, int kc, const void* tw, unsigned long long* umax,
+                 cudaStream_t st) {
+    using F = RowPairs<N>;
+    k_row_max<T, N><<<(N / 2) / F::B, F::THREADS, F::smem_bytes(sizeof(Pair<T>)), st>>>(
+        (const Pair<T>*)X, kc, (const cplx<T>*)tw, umax);
+    return cudaGetLastError();
+}
+
+template <typename T, int N, int STAGE>
+cudaError_t col_stage(void* X, int kc, void* u0t, void* acct, const void* tab, const void* P,
+                      const void* tw, cudaStream_t st) {
+    using F = Fused2D<N>;
+    const int grid = (kc + F::B - 1) / F::B;
+    k_col_pass<T, N, STAGE><<<grid, F::THREADS, F::template smem_bytes<Pair<T>>(), st>>>(
+        (Pair<T>*)X, kc, (cplx<T>*)u0t, (cplx<T>*)acct, (const T*)tab,
+        (const StepParams<T>*)P, (const cplx<T>*)tw);
+    return cudaGetLastError();
+}
+
+template <typename T, int N>
+cudaError_t col(int stage, void* X, int kc, void* u0t, void* acct, const void* tab,
+                const void* P, const void* tw, cudaStream_t st) {
+    switch (stage) {
+        case -1: return col_stage<T, N, -1>(X, kc, u0t, acct, tab, P, tw, st);
+        case 0: return col_stage<T, N, 0>(X, kc, u0t, acct, tab, P, tw, st);
+        case 1: return col_stage<T, N, 1>(X, kc, u0t, acct, tab, P, tw, st);
+        case 2: return col_stage<T, N, 2>(X, kc, u0t, acct, tab, P, tw, st);
+        case 3: return col_stage<T, N, 3>(X, kc, u0t, acct, tab, P, tw, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// Calls F.operator()<T, N>() for the runtime (n, fp64).
+template <typename Fn>
+cudaError_t dispatch(int n, int fp64, Fn&& fn) {
+    if (fp64) {
+        switch (n) {
+            case 16: return fn.template operator()<double, 16>();
+            case 32: return fn.template operator()<double, 32>();
+            case 64: return fn.template operator()<double, 64>();
+            case 128: return fn.template operator()<double, 128>();
+            case 256: return fn.template operator()<double, 256>();
+            case 512: return fn.template operator()<double, 512>();
+            case 1024: return fn.template operator()<double, 1024>();
+            case 2048: return fn.template operator()<double, 2048>();
+            case 4096: return fn.template operator()<double, 4096>();
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (n) {
+        case 16: return fn.template operator()<float, 16>();
+        case 32: return fn.template operator()<float, 32>();
+        case 64: return fn.template operator()<float, 64>();
+        case 128: return fn.template operator()<float, 128>();
+        case 256: return fn.template operator()<float, 256>();
+        case 512: return fn.template operator()<float, 512>();
+        case 1024: return fn.template operator()<float, 1024>();
+        case 2048: return fn.template operator()<float, 2048>();
+        case 4096: return fn.template operator()<float, 4096>();
+        case 8192: return fn.template operator()<float, 8192>();
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+bool supported(int n, int fp64) {
+    if (n < 16 || (n & (n - 1))) return false;
+    return fp64 ? n <= 4096 : n <= 8192;
+}
+
+cudaError_t set_attributes(int n, int fp64) {
+    return dispatch(n, fp64, [&]<typename T, int N>() { return attrs<T, N>(); });
+}
+
+cudaError_t row_pass(int n, int fp64, void* X, int kc, const void* tw, cudaStream_t st) {
+    return dispatch(n, fp64, [&]<typename T, int N>() { return row<T, N>(X, kc, tw, st); });
+}
+
+cudaError_t row_max(int n, int fp64, const void* X, int kc, const void* tw,
+                    unsigned long long* umax, cudaStream_t st) {
+    return dispatch(n, fp64,
+                    [&]<typename T, int N>() { return rmax<T, N>(X, kc, tw, umax, st); });
+}
+
+cudaError_t col_pass(int n, int fp64, int stage, void* X, int kc, void* u0t, void* acct,
+                     const void* tab, const void* params, const void* tw, cudaStream_t st) {
+    return dispatch(n, fp64, [&]<typename T, int N>() {
+        return col<T, N>(stage, X, kc, u0t, acct, tab, params, tw, st);
+    });
+}
+
+cudaError_t transpose_in(int fp64, const void* u0, void* u0t, int n, int kc, cudaStream_t st) {
+    dim3 grid((kc + 31) / 32, (n + 31) / 32), block(32, 8);
+    const int nh = n / 2 + 1;
+    if (fp64)
+        k_transpose_in<double><<<grid, block, 0, st>>>((const cplx<double>*)u0,
+                                                       (cplx<double>*)u0t, n, nh, kc);
+    else
+        k_transpose_in<float><<<grid, block, 0, st>>>((const cplx<float>*)u0, (cplx<float>*)u0t,
+                                                      n, nh, kc);
+    return cudaGetLastError();
+}
+
+cudaError_t transpose_out(int fp64, const void* u0t, void* u0, int n, int kc, cudaStream_t st) {
+    dim3 grid((kc + 31) / 32, (n + 31) / 32), block(32, 8);
+    const int nh = n / 2 + 1;
+    if (fp64)
+        k_transpose_out<double><<<grid, block, 0, st>>>((const cplx<double>*)u0t,
+                                                        (cplx<double>*)u0, n, nh, kc);
+    else
+        k_transpose_out<float><<<grid, block, 0, st>>>((const cplx<float>*)u0t,
+                                                       (cplx<float>*)u0, n, nh, kc);
+    return cudaGetLastError();
+}
+
+cudaError_t mask2d(int fp64, void* u0, int n, cudaStream_t st) {
+    const int nh = n / 2 + 1;
+    const uint32_t fsc = (uint32_t)n * (uint32_t)nh;
+    const unsigned grid = (fsc + 255) / 256;
+    if (fp64) k_mask2d<double><<<grid, 256, 0, st>>>((cplx<double>*)u0, n, nh, fsc);
+    else k_mask2d<float><<<grid, 256, 0, st>>>((cplx<float>*)u0, n, nh, fsc);
+    return cudaGetLastError();
+}
+
+}  // namespace fused
+}  // namespace sp

@@ -1,0 +1,312 @@
+// Fused 2D IF-RK4 stage on hand-written FFTs: two HBM round trips per stage.
+//
+// Only the dealiased columns ky < kc (kc = number of ky with 3 ky < n, about n/3) are ever
+// non-zero in the transforms' inputs or needed from their outputs, so the work array keeps
+// just those: X holds (n rows x kc columns) of Pair<T> — at stage boundaries the pair
+// (u~, v~)(x, ky) of the two velocity fields transformed back along x only; after a row pass
+// the products (P~, Q~)(x, ky) transformed forward along y only.  Rows are interleaved in
+// pairs, X[x/2][ky][x%2] (xidx): a column access then moves whole 32-byte sectors (rows x and
+// x+1 of one column are adjacent) and a row-pair access is contiguous.
+//
+// Row pass (one CTA sub-block per row pair, both rows transformed together as a Pair):
+//   Z(k) = U(k) + i V(k) (Hermitian completion of both half spectra), z = IFFT_n(Z) gives
+//   z = u + i v; the products (v^2 - u^2) + i (u v) are formed in registers; Z' = FFT_n of
+//   that; P(k) = (Z'(k) + conj Z'(n-k)) / 2, Q(k) = (Z'(k) - conj Z'(n-k)) / 2i for k < kc.
+//   One complex transform pair per row replaces the two C2R + two R2C of the reference stage.
+// Column pass (one sub-block per column ky):
+//   forward FFT along x of (P~, Q~) -> (P, Q)(kx, ky); in registers: nonlinear term
+//   N = kx ky P + (kx^2 - ky^2) Q (dealiased), Lawson stage update of the state and the
+//   accumulator, next inputs u = i ky psi, v = -i kx psi (scaled by 1/n^2); inverse FFT along x
+//   -> X.  State and accumulator are kept transposed (ky-major, u0t[ky][x], acct[ky][x]) so the
+//   column pass reads them contiguously; the NumPy-layout state u0 is refreshed on demand.
+#pragma once
+
+#include "common.cuh"
+#include "fft_block.cuh"
+
+namespace sp {
+
+// sub-blocks (rows or columns) per CTA: at least 256 threads per CTA, at most N sub-blocks
+template <int N>
+struct Fused2D {
+    static constexpr int T = N / 16;
+    static constexpr int B = T >= 256 ? 1 : (256 / T < N ? 256 / T : N);
+    static constexpr int THREADS = T * B;
+    template <typename E>
+    static constexpr size_t smem_bytes() { return (size_t)B * FftPlan<N>::SMEM * sizeof(E); }
+};
+
+// Index of element (x, ky) in the row-pair interleaved work array, in Pair<T> units.
+__device__ __forceinline__ size_t xidx(int x, int ky, int kc) {
+    return ((size_t)(x >> 1) * kc + ky) * 2 + (x & 1);
+}
+
+// ------------------------------------------------------------------------------- row pass
+// Z(k) of one row from its stored (U, V)(k): Hermitian completion of both half spectra.
+template <typename T, int N>
+__device__ __forceinline__ cplx<T> row_input(const Pair<T>* __restrict__ X, int p, int k,
+                                             int kc, int half) {
+    if (k < kc) {
+        Pair<T> q = X[((size_t)p * kc + k) * 2 + half];
+        if (k == 0) return mk<T>(q.a.x, q.b.x);  // c2r ignores Im at k = 0
+        return mk<T>(q.a.x - q.b.y, q.a.y + q.b.x);
+    }
+    if (k > N - kc) {
+        Pair<T> q = X[((size_t)p * kc + (N - k)) * 2 + half];
+        return mk<T>(q.a.x + q.b.y, q.b.x - q.a.y);
+    }
+    return mk<T>(0, 0);
+}
+
+// Row pairs per CTA: the sub-block structure of Fused2D over n/2 row pairs.
+template <int N>
+struct RowPairs {
+    static constexpr int T = N / 16;
+    static constexpr int B = T >= 256 ? 1 : (256 / T < N / 2 ? 256 / T : N / 2);
+    static constexpr int THREADS = T * B;
+    static constexpr size_t smem_bytes(size_t elem) { return (size_t)B * FftPlan<N>::SMEM * elem; }
+};
+
+template <typename T, int N>
+__global__ void __launch_bounds__(RowPairs<N>::THREADS) k_row_pass(Pair<T>* __restrict__ X,
+                                                                  int kc,
+                                                                  const cplx<T>* __restrict__ tw) {
+    using F = RowPairs<N>;
+    constexpr int TT = F::T;
+    constexpr int RI = first_radix<N, true>();   // inverse input pattern
+    constexpr int RF = last_radix<N, false>();   // forward output pattern
+    static_assert(last_radix<N, true>() == first_radix<N, false>(), "register hand-off");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int sub = threadIdx.x / TT, t = threadIdx.x % TT;
+    Pair<T>* sm = reinterpret_cast<Pair<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
+    const int p = blockIdx.x * F::B + sub;  // row pair: rows 2p (.a) and 2p + 1 (.b)
+
+    Pair<T> v[16];
+#pragma unroll
+    for (int g = 0; g < 16 / RI; ++g)
+#pragma unroll
+        for (int m = 0; m < RI; ++m) {
+            const int k = in_pos<N, RI>(t, g, m);
+            v[g * RI + m] = Pair<T>{row_input<T, N>(X, p, k, kc, 0), row_input<T, N>(X, p, k, kc, 1)};
+        }
+    block_fft<N, true>(v, sm, t, tw);
+    // physical space, each row: z = u + i v  ->  (v^2 - u^2) + i (u v)
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        T u = v[e].a.x, w = v[e].a.y;
+        v[e].a = mk<T>((w - u) * (w + u), u * w);
+        u = v[e].b.x;
+        w = v[e].b.y;
+        v[e].b = mk<T>((w - u) * (w + u), u * w);
+    }
+    __syncthreads();
+    block_fft<N, false>(v, sm, t, tw);
+    __syncthreads();
+#pragma unroll
+    for (int g = 0; g < 16 / RF; ++g)
+#pragma unroll
+        for (int m = 0; m < RF; ++m) sm[spad(in_pos<N, RF>(t, g, m))] = v[g * RF + m];
+    __syncthreads();
+    // P(k) = (Z'(k) + conj Z'(n-k)) / 2, Q(k) = (Z'(k) - conj Z'(n-k)) / 2i, for each row
+    for (int k = t; k < kc; k += TT) {
+        Pair<T> a = sm[spad(k)], b = sm[spad((N - k) & (N - 1))];
+        Pair<T> o0, o1;
+        o0.a = mk<T>((T)0.5 * (a.a.x + b.a.x), (T)0.5 * (a.a.y - b.a.y));
+        o0.b = mk<T>((T)0.5 * (a.a.y + b.a.y), (T)0.5 * (b.a.x - a.a.x));
+        o1.a = mk<T>((T)0.5 * (a.b.x + b.b.x), (T)0.5 * (a.b.y - b.b.y));
+        o1.b = mk<T>((T)0.5 * (a.b.y + b.b.y), (T)0.5 * (b.b.x - a.b.x));
+        Pair<T>* dst = X + ((size_t)p * kc + k) * 2;
+        dst[0] = o0;
+        dst[1] = o1;
+    }
+}
+
+// CFL bound from the stage-0 inputs: max |u|, max |v| over the physical rows (no write-back).
+template <typename T, int N>
+__global__ void __launch_bounds__(RowPairs<N>::THREADS) k_row_max(const Pair<T>* __restrict__ X,
+                                                                 int kc,
+                                                                 const cplx<T>* __restrict__ tw,
+                                                                 unsigned long long* umax) {
+    using F = RowPairs<N>;
+    constexpr int TT = F::T;
+    constexpr int RI = first_radix<N, true>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int sub = threadIdx.x / TT, t = threadIdx.x % TT;
+    Pair<T>* sm = reinterpret_cast<Pair<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
+    const int p = blockIdx.x * F::B + sub;
+    Pair<T> v[16];
+#pragma unroll
+    for (int g = 0; g < 16 / RI; ++g)
+#pragma unroll
+        for (int m = 0; m < RI; ++m) {
+            const int k = in_pos<N, RI>(t, g, m);
+            v[g * RI + m] = Pair<T>{row_input<T, N>(X, p, k, kc, 0), row_input<T, N>(X, p, k, kc, 1)};
+        }
+    block_fft<N, true>(v, sm, t, tw);
+    double mu = 0.0, mv = 0.0;
+    bool nan_u = false, nan_v = false;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        const double a0 = (double)v[e].a.x, b0 = (double)v[e].a.y;
+        const double a1 = (double)v[e].b.x, b1 = (double)v[e].b.y;
+        nan_u |= (a0 != a0) || (a1 != a1);
+        nan_v |= (b0 != b0) || (b1 != b1);
+        mu = fmax(mu, fmax(fabs(a0), fabs(a1)));
+        mv = fmax(mv, fmax(fabs(b0), fabs(b1)));
+    }
+    unsigned long long bu = (unsigned long long)__double_as_longlong(mu);
+    unsigned long long bv = (unsigned long long)__double_as_longlong(mv);
+    // a NaN anywhere wins the max, as in a NaN-propagating maximum
+    if (nan_u) bu = 0x7ff8000000000000ull;
+    if (nan_v) bv = 0x7ff8000000000000ull;
+    if constexpr (F::THREADS % 32 == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            bu = max(bu, __shfl_down_sync(0xffffffffu, bu, o));
+            bv = max(bv, __shfl_down_sync(0xffffffffu, bv, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMax(umax + 0, bu);
+            atomicMax(umax + 1, bv);
+        }
+    } else {  // tiny grids: a partial warp, no shuffles
+        atomicMax(umax + 0, bu);
+        atomicMax(umax + 1, bv);
+    }
+}
+
+// ------------------------------------------------------------------------------- column pass
+// Next inverse-FFT inputs (u, v) of a vorticity mode, scaled and dealiased (velocity2).
+template <typename T>
+__device__ __forceinline__ Pair<T> next_inputs(T kx, T ky, T k2, bool keep, cplx<T> w, T scale) {
+    T ik2 = (keep && k2 > (T)0) ? scale / k2 : (T)0;
+    cplx<T> psi = scl(ik2, w);
+    Pair<T> o;
+    o.a = scl(ky, mul_i(psi));
+    o.b = scl(kx, mul_mi(psi));
+    return o;
+}
+
+// STAGE 0..3: Lawson stage; STAGE = -1: set-up (no forward transform, no update: the inputs of
+// stage 0 from the state u0t).
+template <typename T, int N, int STAGE>
+__global__ void __launch_bounds__(Fused2D<N>::THREADS) k_col_pass(
+    Pair<T>* __restrict__ X, int kc, cplx<T>* __restrict__ u0t, cplx<T>* __restrict__ acct,
+    const T* __restrict__ tab, const StepParams<T>* __restrict__ P,
+    const cplx<T>* __restrict__ tw) {
+    using F = Fused2D<N>;
+    constexpr int TT = F::T;
+    constexpr int RF0 = first_radix<N, false>();  // forward input pattern
+    constexpr int RL = last_radix<N, false>();    // forward output = inverse input pattern
+    constexpr int RIL = last_radix<N, true>();    // inverse output pattern
+    static_assert(first_radix<N, true>() == RL, "register hand-off");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int sub = threadIdx.x / TT, t = threadIdx.x % TT;
+    Pair<T>* sm = reinterpret_cast<Pair<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
+    const int ky = blockIdx.x * F::B + sub;
+    const bool active = ky < kc;  // inactive sub-blocks still take part in every barrier
+    const StepParams<T> p = *P;
+    const T kyr = (T)ky;
+    const int nh = N / 2 + 1;
+
+    Pair<T> v[16];
+    if constexpr (STAGE >= 0) {
+#pragma unroll
+        for (int g = 0; g < 16 / RF0; ++g)
+#pragma unroll
+            for (int m = 0; m < RF0; ++m) {
+                const int x = in_pos<N, RF0>(t, g, m);
+                v[g * RF0 + m] = active ? X[xidx(x, ky, kc)] : Pair<T>{mk<T>(0, 0), mk<T>(0, 0)};
+            }
+        block_fft<N, false>(v, sm, t, tw);
+    }
+    // v[g*RL + m] now belongs to row index i = in_pos<N, RL>(t, g, m)
+#pragma unroll
+    for (int g = 0; g < 16 / RL; ++g)
+#pragma unroll
+        for (int m = 0; m < RL; ++m) {
+            const int i = in_pos<N, RL>(t, g, m);
+            const int kxi = signed_k(i, N);
+            const int akx = kxi < 0 ? -kxi : kxi;
+            const bool keep = active && (3 * akx < N);
+            const T kx = (T)kxi, k2 = kx * kx + kyr * kyr;
+            cplx<T> nxt = mk<T>(0, 0);
+            if (keep) {
+                const size_t o = (size_t)ky * N + i;
+                cplx<T> U = u0t[o];
+                if constexpr (STAGE < 0) {
+                    nxt = U;
+                } else {
+                    Pair<T> e = v[g * RL + m];
+                    cplx<T> Nl = axpy(kx * kyr, e.a, scl(kx * kx - kyr * kyr, e.b));
+                    IFac<T> f = if_factors(tab, nh, akx, ky, -1, k2, p);
+                    cplx<T> C = STAGE > 0 ? acct[o] : mk<T>(0, 0);
+                    nxt = lawson_stage<T, (STAGE < 0 ? 0 : STAGE)>(p.dt, f, Nl, U, C);
+                    if (STAGE == 3) u0t[o] = nxt;
+                    else acct[o] = C;
+                }
+            }
+            v[g * RL + m] = next_inputs<T>(kx, kyr, k2, keep, nxt, p.scale);
+        }
+    __syncthreads();
+    block_fft<N, true>(v, sm, t, tw);
+    if (active) {
+#pragma unroll
+        for (int g = 0; g < 16 / RIL; ++g)
+#pragma unroll
+            for (int m = 0; m < RIL; ++m) {
+                const int x = in_pos<N, RIL>(t, g, m);
+                X[xidx(x, ky, kc)] = v[g * RIL + m];
+            }
+    }
+}
+
+// ------------------------------------------------------------------------------- layout moves
+// u0 (n, nh) NumPy layout -> u0t (kc, n): 32 x 32 tiles through shared memory.
+template <typename T>
+__global__ void __launch_bounds__(256) k_transpose_in(const cplx<T>* __restrict__ u0,
+                                                      cplx<T>* __restrict__ u0t, int n, int nh,
+                                                      int kc) {
+    __shared__ cplx<T> tile[32][33];
+    const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;  // i = row (x index), j = ky
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        int i = i0 + r, j = j0 + threadIdx.x;
+        tile[r][threadIdx.x] = (i < n && j < kc) ? u0[(size_t)i * nh + j] : mk<T>(0, 0);
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        int j = j0 + r, i = i0 + threadIdx.x;
+        if (j < kc && i < n) u0t[(size_t)j * n + i] = tile[threadIdx.x][r];
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_transpose_out(const cplx<T>* __restrict__ u0t,
+                                                       cplx<T>* __restrict__ u0, int n, int nh,
+                                                       int kc) {
+    __shared__ cplx<T> tile[32][33];
+    const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        int j = j0 + r, i = i0 + threadIdx.x;
+        tile[r][threadIdx.x] = (j < kc && i < n) ? u0t[(size_t)j * n + i] : mk<T>(0, 0);
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += 8) {
+        int i = i0 + r, j = j0 + threadIdx.x;
+        if (i < n && j < kc) u0[(size_t)i * nh + j] = tile[threadIdx.x][r];
+    }
+}
+
+// dealias a 2D state in place (zero every mode outside 3|kx| < n, 3 ky < n)
+template <typename T>
+__global__ void __launch_bounds__(256) k_mask2d(cplx<T>* __restrict__ u0, int n, int nh,
+                                                uint32_t fsc) {
+    uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= fsc) return;
+    uint32_t i = idx / (uint32_t)nh, j = idx - i * (uint32_t)nh;
+    int kxi = signed_k((int)i, n);
+    int akx = kxi < 0 ? -kxi : kxi;
+    if (!(3 * akx < n && 3 * (int)j < n)) u0[idx] = mk<T>(0, 0);
+}
+
+}  // namespace sp

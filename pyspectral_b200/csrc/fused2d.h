@@ -1,0 +1,29 @@
+// Host launchers of the fused 2D engine (kernels in fused2d.cuh, compiled in fused2d.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sp {
+namespace fused {
+
+// True when the fused 2D engine has kernels for grid n in this precision
+// (n a power of two, 16 <= n <= 8192 in fp32, <= 4096 in fp64).
+bool supported(int n, int fp64);
+// Number of dealiased ky columns kept by the transforms: ky with 3 ky < n.
+inline int kc_of(int n) { return (n + 2) / 3; }
+// Opt every kernel of this size into its dynamic shared memory; once per process and size.
+cudaError_t set_attributes(int n, int fp64);
+
+cudaError_t row_pass(int n, int fp64, void* X, int kc, const void* tw, cudaStream_t st);
+cudaError_t row_max(int n, int fp64, const void* X, int kc, const void* tw,
+                    unsigned long long* umax, cudaStream_t st);
+// stage -1: build the stage-0 inputs from u0t; 0..3: Lawson stage
+cudaError_t col_pass(int n, int fp64, int stage, void* X, int kc, void* u0t, void* acct,
+                     const void* tab, const void* params, const void* tw, cudaStream_t st);
+cudaError_t transpose_in(int fp64, const void* u0, void* u0t, int n, int kc, cudaStream_t st);
+cudaError_t transpose_out(int fp64, const void* u0t, void* u0, int n, int kc, cudaStream_t st);
+cudaError_t mask2d(int fp64, void* u0, int n, cudaStream_t st);
+
+}  // namespace fused
+}  // namespace sp

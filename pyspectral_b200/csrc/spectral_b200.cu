@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "spectral_b200.h"
+#include "fused2d.h"
 #include "pointwise.cuh"
 #include "reduce.cuh"
 
@@ -67,7 +68,13 @@ struct sp_solver {
     bool bound = false;
     // aux sub-blocks
     size_t off_params = 0, off_tab = 0, off_partials = 0, off_umax = 0, off_out = 0, off_spec = 0;
+    size_t off_tw = 0;
     size_t aux_bytes = 0;
+    // fused 2D mode: kept ky columns, work-array split (X then the transposed state u0t) and
+    // whether the NumPy-layout state u0 reflects the transposed state
+    int kc = 0;
+    size_t work_bytes = 0, off_u0t = 0;
+    bool u0_fresh = true;
     // cuFFT
     cufftHandle plan_inv = 0, plan_fwd = 0, plan_c2r1 = 0;
     bool have_inv = false, have_fwd = false, have_c2r1 = false;
@@ -93,6 +100,9 @@ struct sp_solver {
     unsigned long long* umax_dev() const { return (unsigned long long*)((char*)aux + off_umax); }
     double* out_dev() const { return (double*)((char*)aux + off_out); }
     double* spec_dev() const { return (double*)((char*)aux + off_spec); }
+    void* tw_dev() const { return (char*)aux + off_tw; }
+    void* u0t_dev() const { return (char*)W + off_u0t; }
+    bool fused() const { return fft_mode == SP_FFT_FUSED; }
 };
 
 namespace {
@@ -308,8 +318,30 @@ int run_post(sp_solver* s, int stage, cudaStream_t st) {
     return s->fp64 ? launch_post<double>(s, stage, st) : launch_post<float>(s, stage, st);
 }
 
-// One IF-RK4 step: 4 x (inverse FFT -> phys -> forward FFT -> post), cupy_cuda.py:163-178.
+int fused_row(sp_solver* s, cudaStream_t st) {
+    SP_CUDA(sp::fused::row_pass(s->n, s->fp64, s->W, s->kc, s->tw_dev(), st));
+    s->launches += 1;
+    return SP_OK;
+}
+
+int fused_col(sp_solver* s, int stage, cudaStream_t st) {
+    SP_CUDA(sp::fused::col_pass(s->n, s->fp64, stage, s->W, s->kc, s->u0t_dev(), s->acc,
+                                s->tab_dev(), s->params_dev(), s->tw_dev(), st));
+    s->launches += 1;
+    return SP_OK;
+}
+
+// One IF-RK4 step: 4 x (inverse FFT -> phys -> forward FFT -> post), cupy_cuda.py:163-178;
+// in the fused mode 4 x (row pass -> column pass).
 int run_step(sp_solver* s, cudaStream_t st) {
+    if (s->fused()) {
+        for (int stage = 0; stage < 4; ++stage) {
+            int r;
+            if ((r = fused_row(s, st))) return r;
+            if ((r = fused_col(s, stage, st))) return r;
+        }
+        return SP_OK;
+    }
     for (int stage = 0; stage < 4; ++stage) {
         int r;
         if ((r = fft_inverse(s, st))) return r;
@@ -375,8 +407,13 @@ sp_solver* sp_create(int n, int dim, int form, int fp64, int fft_mode, int* stat
         return set(SP_ERR_ARG, "unknown form");
     if (dim == 2 && form != SP_FORM_BASDEVANT)
         return set(SP_ERR_UNSUPPORTED, "2D supports the basdevant form only");
-    if (fft_mode != SP_FFT_CUFFT && fft_mode != SP_FFT_CUFFT_LEAN)
+    if (fft_mode != SP_FFT_CUFFT && fft_mode != SP_FFT_CUFFT_LEAN && fft_mode != SP_FFT_FUSED)
         return set(SP_ERR_ARG, "unknown fft_mode");
+    if (fft_mode == SP_FFT_FUSED && dim != 2)
+        return set(SP_ERR_UNSUPPORTED, "the fused FFT engine runs 2D grids only");
+    if (fft_mode == SP_FFT_FUSED && !sp::fused::supported(n, fp64))
+        return set(SP_ERR_UNSUPPORTED,
+                   "the fused FFT engine needs n a power of two in 16..8192 (fp32) or 16..4096 (fp64)");
     int nh = n / 2 + 1;
     uint64_t fsc = (uint64_t)nh * (uint64_t)n * (dim == 3 ? (uint64_t)n : 1ull);
     if (2 * fsc >= (1ull << 32)) return set(SP_ERR_ARG, "grid too large for 32-bit indexing");
@@ -409,7 +446,23 @@ sp_solver* sp_create(int n, int dim, int form, int fp64, int fft_mode, int* stat
     s->off_umax = off; off += align256(4 * sizeof(unsigned long long));
     s->off_out = off; off += align256(8 * sizeof(double));
     s->off_spec = off; off += align256((size_t)s->nshell * sizeof(double));
+    s->off_tw = off; off += align256((size_t)n * 2 * s->rsize);
     s->aux_bytes = off;
+    s->work_bytes = (size_t)s->nwork * field_bytes(s);
+
+    if (fft_mode == SP_FFT_FUSED) {
+        s->kc = sp::fused::kc_of(n);
+        size_t csz = 2 * s->rsize;
+        s->off_u0t = align256((size_t)n * s->kc * 2 * csz);         // X: n x kc pairs
+        s->work_bytes = s->off_u0t + align256((size_t)s->kc * n * csz);  // + u0t: kc x n
+        cudaError_t e = sp::fused::set_attributes(n, fp64);
+        if (e != cudaSuccess) {
+            sp_destroy(s);
+            return set(SP_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+        }
+        if (status) *status = SP_OK;
+        return s;
+    }
 
     bool lean = fft_mode == SP_FFT_CUFFT_LEAN;
     size_t ws_inv = 0, ws_fwd = 0, ws_one = 0;
@@ -450,7 +503,7 @@ int sp_query_sizes(const sp_solver* s, int64_t* out, int count) {
     v[SP_SZ_NINV] = s->ninv;
     v[SP_SZ_NFWD] = s->nfwd;
     v[SP_SZ_STATE_BYTES] = (int64_t)s->ncomp * (int64_t)field_bytes(s);
-    v[SP_SZ_WORK_BYTES] = (int64_t)s->nwork * (int64_t)field_bytes(s);
+    v[SP_SZ_WORK_BYTES] = (int64_t)s->work_bytes;
     v[SP_SZ_AUX_BYTES] = (int64_t)s->aux_bytes;
     v[SP_SZ_FFTWS_BYTES] = (int64_t)s->ws_bytes;
     v[SP_SZ_NSHELL] = s->nshell;
@@ -469,7 +522,7 @@ int sp_bind(sp_solver* s, void* u0, void* acc, void* work, void* aux, void* fft_
     s->W = work;
     s->aux = aux;
     s->fftws = fft_workspace;
-    if (s->ws_bytes) {
+    if (s->ws_bytes && !s->fused()) {
         SP_CUFFT(cufftSetWorkArea(s->plan_inv, fft_workspace));
         SP_CUFFT(cufftSetWorkArea(s->plan_fwd, fft_workspace));
         if (s->have_c2r1) SP_CUFFT(cufftSetWorkArea(s->plan_c2r1, fft_workspace));
@@ -478,6 +531,24 @@ int sp_bind(sp_solver* s, void* u0, void* acc, void* work, void* aux, void* fft_
     s->tab_valid = false;
     s->params_valid = false;
     drop_graph(s);
+    if (s->fused()) {
+        // twiddle table tw[i] = exp(+2 pi i i / n), fp64 on the host, rounded to the real type
+        std::vector<double> tw(2 * (size_t)s->n);
+        for (int i = 0; i < s->n; ++i) {
+            double a = 2.0 * M_PI * (double)i / (double)s->n;
+            tw[2 * i] = std::cos(a);
+            tw[2 * i + 1] = std::sin(a);
+        }
+        if (s->fp64) {
+            SP_CUDA(cudaMemcpy(s->tw_dev(), tw.data(), tw.size() * sizeof(double),
+                               cudaMemcpyHostToDevice));
+        } else {
+            std::vector<float> twf(tw.begin(), tw.end());
+            SP_CUDA(cudaMemcpy(s->tw_dev(), twf.data(), twf.size() * sizeof(float),
+                               cudaMemcpyHostToDevice));
+        }
+        s->u0_fresh = true;
+    }
     return SP_OK;
 }
 
@@ -506,7 +577,25 @@ int sp_prepare(sp_solver* s, void* stream) {
         int r = upload_params(s, s->tab_valid ? s->tab_dt : 0.0, st);
         if (r) return r;
     }
+    if (s->fused()) {
+        SP_CUDA(sp::fused::mask2d(s->fp64, s->u0, s->n, st));
+        SP_CUDA(sp::fused::transpose_in(s->fp64, s->u0, s->u0t_dev(), s->n, s->kc, st));
+        s->launches += 2;
+        int r = fused_col(s, -1, st);
+        s->u0_fresh = true;
+        return r;
+    }
     return run_pre(s, st);
+}
+
+int sp_sync_state(sp_solver* s, void* stream) {
+    SP_CHECK_BOUND(s);
+    if (!s->fused() || s->u0_fresh) return SP_OK;
+    SP_CUDA(sp::fused::transpose_out(s->fp64, s->u0t_dev(), s->u0, s->n, s->kc,
+                                     (cudaStream_t)stream));
+    s->launches += 1;
+    s->u0_fresh = true;
+    return SP_OK;
 }
 
 int sp_set_graph(sp_solver* s, int enable) {
@@ -521,6 +610,7 @@ int sp_step(sp_solver* s, double dt, void* stream) {
     auto st = (cudaStream_t)stream;
     int r = upload_params(s, dt, st);
     if (r) return r;
+    if (s->fused()) s->u0_fresh = false;
     if (!s->graph_on) return run_step(s, st);
     if (!s->exec && (r = capture_step(s))) return r;
     SP_CUDA(cudaGraphLaunch(s->exec, st));
@@ -532,6 +622,16 @@ int sp_run_phase(sp_solver* s, int phase, int stage, void* stream) {
     SP_CHECK_BOUND(s);
     auto st = (cudaStream_t)stream;
     if (stage < 0 || stage > 3) return fail(s, SP_ERR_ARG, "sp_run_phase", "stage must be 0..3");
+    if (s->fused()) {
+        if (phase < 0 || phase > 3) return fail(s, SP_ERR_ARG, "sp_run_phase", "phase must be 0..3");
+        if (phase == 0) return fused_row(s, st);
+        if (phase == 3) {
+            if (!s->params_valid) return fail(s, SP_ERR_STATE, "sp_run_phase", "no step parameters yet");
+            s->u0_fresh = false;
+            return fused_col(s, stage, st);
+        }
+        return SP_OK;  // phases 1 and 2 live inside the row pass
+    }
     switch (phase) {
         case 0: return fft_inverse(s, st);
         case 1: return run_phys(s, st);
@@ -548,6 +648,10 @@ int sp_diagnostics(sp_solver* s, const void* state, double band_klo, double band
     SP_CHECK_BOUND(s);
     if (!state || !out) return fail(s, SP_ERR_ARG, "sp_diagnostics", "null pointer");
     auto st = (cudaStream_t)stream;
+    if (state == s->u0) {
+        int r = sp_sync_state(s, stream);
+        if (r) return r;
+    }
     double norm = std::pow((double)s->n, 2.0 * s->dim);
     double w_edge = 1.0 / norm, w_mid = 2.0 / norm;
     unsigned g = grid_for(s->fsc, kRedThreads);
@@ -576,6 +680,28 @@ int sp_max_velocity(sp_solver* s, const void* state, double* out_sum, double* ou
     if (!state || !out_sum) return fail(s, SP_ERR_ARG, "sp_max_velocity", "null pointer");
     auto st = (cudaStream_t)stream;
     int ncomp = s->dim;  // velocity components
+    if (s->fused()) {
+        // the work array holds the stage-0 inputs of the live state: one inverse row pass
+        if (state != s->u0)
+            return fail(s, SP_ERR_UNSUPPORTED, "sp_max_velocity",
+                        "the fused engine bounds the velocity of its own state only");
+        SP_CUDA(cudaMemsetAsync(s->umax_dev(), 0, 4 * sizeof(unsigned long long), st));
+        SP_CUDA(sp::fused::row_max(s->n, s->fp64, s->W, s->kc, s->tw_dev(), s->umax_dev(), st));
+        s->launches += 1;
+        unsigned long long bits[4] = {0, 0, 0, 0};
+        SP_CUDA(cudaMemcpyAsync(bits, s->umax_dev(), sizeof(bits), cudaMemcpyDeviceToHost, st));
+        SP_CUDA(cudaStreamSynchronize(st));
+        double sum = 0.0;
+        for (int c = 0; c < 2; ++c) {
+            double v;
+            std::memcpy(&v, &bits[c], sizeof(v));
+            if (out_per_comp) out_per_comp[c] = v;
+            sum += v;
+        }
+        if (out_per_comp) out_per_comp[2] = 0.0;
+        *out_sum = sum;
+        return SP_OK;
+    }
     cufftHandle plan = s->fft_mode == SP_FFT_CUFFT_LEAN ? s->plan_inv : s->plan_c2r1;
     SP_CUDA(cudaMemsetAsync(s->umax_dev(), 0, 4 * sizeof(unsigned long long), st));
     unsigned gv = grid_for(s->fsc, kRedThreads);
@@ -626,6 +752,10 @@ int sp_spectrum(sp_solver* s, const void* state, double* out, int nshell, void* 
     if (!state || !out) return fail(s, SP_ERR_ARG, "sp_spectrum", "null pointer");
     if (nshell != s->nshell) return fail(s, SP_ERR_ARG, "sp_spectrum", "nshell mismatch");
     auto st = (cudaStream_t)stream;
+    if (state == s->u0) {
+        int r = sp_sync_state(s, stream);
+        if (r) return r;
+    }
     double norm = std::pow((double)s->n, 2.0 * s->dim);
     SP_CUDA(cudaMemsetAsync(s->spec_dev(), 0, (size_t)nshell * sizeof(double), st));
     unsigned g = grid_for(s->fsc, kRedThreads);

@@ -65,6 +65,9 @@ def register(registry: list | None = None) -> list[Any]:
         B200Variant("b200", "fused-inplace-graph", "pyspectral_b200.solver", "B200Solver",
                     "#17becf", True, "B200, whole step in one CUDA graph, device-resident dt",
                     default=True),
+        B200Variant("b200", "fused-fft-graph", "pyspectral_b200.solver", "B200FusedSolver",
+                    "#17becf", True, "B200 2D, hand-written FFTs fused with the pointwise "
+                    "phases, no cuFFT"),
     ]
     have = {v.name for v in reg}
     added = [e for e in entries if e.name not in have]

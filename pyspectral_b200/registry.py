@@ -58,6 +58,9 @@ REGISTRY: list[Variant] = [
     Variant("b200", "fused-inplace-graph", "solver", "B200Solver", True,
             "as above, batched plans, whole step replayed from one CUDA graph with "
             "device-resident dt/forcing", default=True),
+    Variant("b200", "fused-fft-graph", "solver", "B200FusedSolver", True,
+            "2D: hand-written sm_100a FFTs fused with every pointwise phase (row pass + column "
+            "pass per RK stage over the dealiased columns), no cuFFT, one CUDA graph per step"),
 ]
 
 

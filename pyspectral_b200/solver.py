@@ -23,7 +23,6 @@ import numpy as np
 from pyspectral_b200 import _lib
 from pyspectral_b200.base import BackendUnavailable, SpectralSolver
 from pyspectral_b200.config import Config, fft_split
-from pyspectral_b200.grid import spectral_shape
 from pyspectral_b200.ops import TorchOps
 
 
@@ -77,19 +76,17 @@ class B200Solver(SpectralSolver):
         self.sizes = list(sizes)
         self.rdt = torch.float64 if fp64 else torch.float32
         self.cdt = torch.complex128 if fp64 else torch.complex64
-        spec = spectral_shape(self.n, self.dim)
         self.n_inv, self.n_fwd = fft_split(self.dim, self.form)
         self.nw = int(sizes[_lib.SZ_NWORK])
         dev = torch.device("cuda", torch.cuda.current_device())
         self.device = dev
         self.u0 = torch.zeros(self.state_shape(), dtype=self.cdt, device=dev)
         self.acc = torch.zeros_like(self.u0)
-        self.W = torch.zeros((self.nw,) + spec, dtype=self.cdt, device=dev)
+        self.W = torch.zeros(int(sizes[_lib.SZ_WORK_BYTES]), dtype=torch.uint8, device=dev)
         self.aux = torch.zeros(int(sizes[_lib.SZ_AUX_BYTES]), dtype=torch.uint8, device=dev)
         self.fftws = torch.empty(max(1, int(sizes[_lib.SZ_FFTWS_BYTES])), dtype=torch.uint8,
                                  device=dev)
         assert self.u0.nbytes == sizes[_lib.SZ_STATE_BYTES]
-        assert self.W.nbytes == sizes[_lib.SZ_WORK_BYTES]
         self._check(lib.sp_bind(h, _lib.dptr(self.u0), _lib.dptr(self.acc), _lib.dptr(self.W),
                                 _lib.dptr(self.aux), _lib.dptr(self.fftws)), "sp_bind")
         self._check(lib.sp_set_physics(h, float(cfg.nu), float(cfg.alpha), float(cfg.drag_k2),
@@ -158,11 +155,14 @@ class B200Solver(SpectralSolver):
     def get_state(self) -> np.ndarray:
         """The state copied to the host as complex128 (through the pinned staging buffer)."""
         stage = self._host_staging()
-        stage.copy_(self.u0, non_blocking=True)
+        stage.copy_(self.state_native(), non_blocking=True)
         self.torch.cuda.current_stream(self.device).synchronize()
         return stage.numpy().astype(np.complex128)
 
     def state_native(self) -> Any:
+        """The live state (NumPy r2c layout).  Engines that advance a transposed copy write it
+        back here first, so the tensor is current when returned."""
+        self._check(self.lib.sp_sync_state(self._h, self._stream()), "sp_sync_state")
         return self.u0
 
     @property
@@ -202,3 +202,15 @@ class B200LeanSolver(B200Solver):
 
     variant = "fused-inplace-lean"
     fft_mode = _lib.FFT_CUFFT_LEAN
+
+
+class B200FusedSolver(B200Solver):
+    """2D: hand-written FFTs fused with the pointwise phases — per RK stage one row pass
+    (inverse row FFT, products, forward row FFT) and one column pass (forward column FFT,
+    Lawson update, inverse column FFT) over the 2/3-dealiased columns; no cuFFT; one CUDA
+    graph per step.  n a power of two, 16..8192 (fp32) or 16..4096 (fp64)."""
+
+    variant = "fused-fft-graph"
+    dims = (2,)
+    forms = ("basdevant",)
+    fft_mode = _lib.FFT_FUSED

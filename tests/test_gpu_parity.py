@@ -29,6 +29,15 @@ def rel(a: np.ndarray, b: np.ndarray) -> float:
     return float(np.abs(a - b).max() / np.abs(b).max())
 
 
+def _make(v, cfg: Config):
+    """Construct variant v, skipping when it does not run this configuration (like the
+    reference's tests/test_backends.py:17-21)."""
+    try:
+        return v.make(cfg)
+    except BackendUnavailable as e:
+        pytest.skip(str(e))
+
+
 def _oracle(cfg: Config, **kw) -> OracleSolver:
     return OracleSolver(cfg.n, cfg.dim, nu=cfg.nu, alpha=cfg.alpha, alpha_kmax=cfg.alpha_kmax,
                         force_amp=cfg.force_amp, force_klo=cfg.force_klo,
@@ -44,7 +53,7 @@ def test_matches_oracle(v, dtype, dim, form, alpha_kmax):
     n = 32 if dim == 2 else 16
     cfg = Config(n=n, dim=dim, nu=0.01, alpha=0.5, alpha_kmax=alpha_kmax, force_amp=0.3,
                  force_klo=1, force_khi=2.5, dtype=dtype, form=form)
-    s = v.make(cfg)
+    s = _make(v, cfg)
     ref = _oracle(cfg)
     ic = (initial.to_spectral(initial.random_2d(n, k0=4), 2) if dim == 2
           else initial.to_spectral(initial.random_3d(n, k0=2), 3))
@@ -79,7 +88,7 @@ def test_matches_reference_vectors(dim, form, akm):
 @pytest.mark.parametrize("v", VARIANTS, ids=lambda v: v.name)
 def test_tgv2d_exact(v):
     n, nu = 32, 0.05
-    s = v.make(Config(n=n, dim=2, nu=nu, dtype="float64"))
+    s = _make(v, Config(n=n, dim=2, nu=nu, dtype="float64"))
     w0 = initial.to_spectral(initial.taylor_green_2d(n), 2)
     s.set_state(w0)
     s.advance(20, 0.05)
@@ -286,3 +295,99 @@ def test_workload_8192_fp32_matches_oracle_one_step():
     ref.set_state(w0)
     ref.step(dt)
     assert rel(s.get_state(), ref.get_state()) < 1e-5
+
+
+# ----------------------------------------------------------------------------- fused FFT engine
+FUSED = "b200/fused-fft-graph"
+
+
+@pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512, 1024, 2048])
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_fused_matches_oracle_every_size(n, dtype):
+    """The hand-written FFT engine against the fp64 oracle at every transform size it
+    instantiates, with drag band, forcing, an amplitude change and a dt change."""
+    cfg = Config(n=n, dim=2, nu=0.01, alpha=0.5, alpha_kmax=2.0, force_amp=0.3, force_klo=1,
+                 force_khi=2.5, dtype=dtype)
+    s = get(FUSED).make(cfg)
+    ref = _oracle(cfg)
+    ic = initial.to_spectral(initial.random_2d(n, k0=min(4, n / 8)), 2)
+    s.set_state(ic)
+    ref.set_state(ic)
+    s.advance(3, 0.01)
+    ref.advance(3, 0.01)
+    s.set_forcing_amplitude(0.1)
+    ref.set_forcing_amplitude(0.1)
+    s.advance(2, 0.007)
+    ref.advance(2, 0.007)
+    assert rel(s.get_state(), ref.get_state()) < TOL[dtype]
+
+
+@pytest.mark.parametrize("n", [4096])
+def test_fused_fp64_matches_cufft_fp64(n):
+    cfg = Config(n=n, dim=2, nu=1e-4, dtype="float64")
+    ic = initial.random_phase_2d(n, k0=12, seed=3)
+    out = []
+    for name in (FUSED, "b200/fused-inplace-graph"):
+        s = get(name).make(cfg)
+        s.set_state(ic)
+        s.advance(2, 2e-4)
+        out.append(s.get_state())
+    assert rel(out[0], out[1]) < 1e-12
+
+
+def test_fused_workload_8192_one_step_vs_oracle():
+    n = 8192
+    w0 = initial.random_phase_2d(n, k0=12, seed=0, energy=0.5)
+    s = get(FUSED).make(Config(n=n, dim=2, nu=2e-6, dtype="float32"))
+    s.set_state(w0)
+    dt = 0.5 * (2 * math.pi / n) / s.diag.max_velocity_sum(s.state_native())
+    s.step(dt)
+    ref = OracleSolver(n, 2, nu=2e-6)
+    ref.set_state(w0)
+    ref.step(dt)
+    assert rel(s.get_state(), ref.get_state()) < 1e-5
+
+
+def test_fused_diagnostics_and_cfl_match_cufft_engine():
+    n = 1024
+    cfg = Config(n=n, dim=2, nu=1e-4, dtype="float64", alpha=0.1, alpha_kmax=2,
+                 force_amp=0.5, force_klo=3, force_khi=5)
+    ic = initial.random_phase_2d(n, k0=10, seed=4)
+    a, b = get(FUSED).make(cfg), get("b200/fused-inplace-graph").make(cfg)
+    for s in (a, b):
+        s.set_state(ic)
+        s.advance(3, 1e-3)
+    da, db = a.diag.all(a.state_native(), 3, 5), b.diag.all(b.state_native(), 3, 5)
+    for k in da:
+        assert da[k] == pytest.approx(db[k], rel=1e-12)
+    ua, pa = a.diag.max_velocity(a.state_native())
+    ub, pb = b.diag.max_velocity(b.state_native())
+    assert ua == pytest.approx(ub, rel=1e-12)
+    ea, eb = a.diag.spectrum(a.state_native())[1], b.diag.spectrum(b.state_native())[1]
+    # shells far past the spectral peak hold round-off (~1e-26): compare against the total
+    np.testing.assert_allclose(ea, eb, rtol=1e-11, atol=1e-14 * eb.sum())
+
+
+def test_fused_graph_replays_every_dt_and_amplitude():
+    cfg = Config(n=256, dim=2, nu=1e-3, alpha=0.1, alpha_kmax=2, force_amp=0.2, force_klo=3,
+                 force_khi=5, dtype="float64")
+    ic = initial.random_phase_2d(256, k0=8, seed=2)
+    s = get(FUSED).make(cfg)
+    ref = _oracle(cfg)
+    s.set_state(ic)
+    ref.set_state(ic)
+    for k in range(6):
+        s.set_forcing_amplitude(0.2 + 0.05 * k)
+        ref.set_forcing_amplitude(0.2 + 0.05 * k)
+        s.step(1e-3 * (1 + 0.3 * k))
+        ref.step(1e-3 * (1 + 0.3 * k))
+    assert rel(s.get_state(), ref.get_state()) < 1e-12
+    launches = s.kernel_launches
+    s.step(1e-3)
+    assert s.kernel_launches - launches == 8  # 4 x (row pass + column pass)
+
+
+def test_fused_rejects_what_it_does_not_run():
+    for cfg in (Config(n=48, dim=2), Config(n=16, dim=3), Config(n=8192, dim=2, dtype="float64")):
+        with pytest.raises(BackendUnavailable):
+            get(FUSED).make(cfg)

@@ -219,7 +219,7 @@ def test_plugin_registers_into_pyspectral_registry(capsys):
     added = register()
     register()  # idempotent
     try:
-        assert len(REF) == before + 3 == before + len(added)
+        assert len(REF) == before + 4 == before + len(added)
         v = ref_get("b200")
         assert v.name == "b200/fused-inplace-graph"
         cls = v.load()
