@@ -11,16 +11,19 @@
 // forward transform starting with radix R without any exchange (and vice versa).
 //
 // Elements are either one complex sequence (cplx<T>) or two sequences sharing the transform
-// (Pair<T>).  Twiddles come from a table tw[i] = exp(+2 pi i i/N) (fp64 on the host, rounded
-// to T); the forward transform conjugates them.  DIR = +1: inverse (e^{+}), DIR = -1: forward.
+// (Pair<T>).  Twiddles come from a per-pass table (FftPlan::tw_offset, built in fp64 on the
+// host and rounded to T); the forward transform conjugates them.  DIR = +1: inverse (e^{+}),
+// DIR = -1: forward.
 #pragma once
 
 #include "common.cuh"
 
 namespace sp {
 
+// Two complex values moved as one unit: aligned to its size so a Pair<float> is one 128-bit
+// access (and a Pair<double> two) instead of separate 64-bit halves.
 template <typename T>
-struct Pair {
+struct alignas(4 * sizeof(T) <= 16 ? 4 * sizeof(T) : 16) Pair {
     cplx<T> a, b;
 };
 
@@ -206,6 +209,22 @@ struct FftPlan {
         for (int q = 0; q < p; ++q) s *= radix(inv, q);
         return s;
     }
+    // Per-pass twiddle table: for the inverse passes p = 1..NP-1, then the forward passes
+    // p = 1..NP-1, a block of 3 S_p entries [w^1 | w^4 | w^8], w = exp(+2 pi i js / (S_p R_p)),
+    // js < S_p.  tw_offset is the start of a pass's block; TW_SIZE the whole table.
+    static constexpr int tw_offset(bool inv, int p) {
+        int o = 0;
+        for (int q = 1; q < NP; ++q) {
+            if (inv && q == p) return o;
+            o += 3 * stride(true, q);
+        }
+        for (int q = 1; q < NP; ++q) {
+            if (!inv && q == p) return o;
+            o += 3 * stride(false, q);
+        }
+        return o;
+    }
+    static constexpr int TW_SIZE = tw_offset(false, NP) > 0 ? tw_offset(false, NP) : 1;
 };
 
 // shared-memory index with one pad element every 16 (conflict-free strided access)
@@ -225,22 +244,24 @@ __device__ __forceinline__ C tw_load(const C* __restrict__ tw, int idx) {
 }
 
 // Twiddles w^m, m = 1..R-1, of one group: three table loads (w, w^4, w^8) and at most three
-// dependent complex products for the others, instead of R-1 scattered table loads.
-template <int R, int DIR, typename C>
-__device__ __forceinline__ void group_twiddles(C (&w)[16], const C* __restrict__ tw, int base) {
-    w[1] = tw_load<DIR>(tw, base);
+// dependent complex products for the others, instead of R-1 scattered table loads.  `tw`
+// points at this pass's block [w^1 | w^4 | w^8] x S of the per-pass table, so the loads of a
+// warp (consecutive js) are contiguous.
+template <int R, int S, int DIR, typename C>
+__device__ __forceinline__ void group_twiddles(C (&w)[16], const C* __restrict__ tw, int js) {
+    w[1] = tw_load<DIR>(tw, js);
     if constexpr (R >= 4) {
         w[2] = cmul(w[1], w[1]);
         w[3] = cmul(w[2], w[1]);
     }
     if constexpr (R >= 8) {
-        w[4] = tw_load<DIR>(tw, 4 * base);
+        w[4] = tw_load<DIR>(tw, S + js);
         w[5] = cmul(w[4], w[1]);
         w[6] = cmul(w[4], w[2]);
         w[7] = cmul(w[4], w[3]);
     }
     if constexpr (R >= 16) {
-        w[8] = tw_load<DIR>(tw, 8 * base);
+        w[8] = tw_load<DIR>(tw, 2 * S + js);
         w[9] = cmul(w[8], w[1]);
         w[10] = cmul(w[8], w[2]);
         w[11] = cmul(w[8], w[3]);
@@ -258,10 +279,10 @@ __device__ __forceinline__ void pass_compute(E (&v)[16], int t, const C* __restr
 #pragma unroll
     for (int g = 0; g < G; ++g) {
         if constexpr (S > 1) {
-            // w_{S R}^{js m} = w_N^{js m N/(S R)}; the index of w^8 stays below N
+            // w_{S R}^{js m}, from this pass's block of the per-pass table
             const int js = (t + T * g) & (S - 1);
             C w[16];
-            group_twiddles<R, DIR>(w, tw, js * (N / (S * R)));
+            group_twiddles<R, S, DIR>(w, tw, js);
 #pragma unroll
             for (int m = 1; m < R; ++m) v[g * R + m] = emul(v[g * R + m], w[m]);
         }
@@ -299,28 +320,28 @@ __device__ __forceinline__ void block_fft(E (&v)[16], E* sm, int t, const C* __r
     using P = FftPlan<N>;
     constexpr int DIR = INV ? 1 : -1;
     constexpr int R0 = P::radix(INV, 0), S0 = P::stride(INV, 0);
-    pass_compute<N, R0, S0, DIR>(v, t, tw);
+    pass_compute<N, R0, S0, DIR>(v, t, tw);  // S0 = 1: no twiddles
     if constexpr (P::NP > 1) {
         constexpr int R1 = P::radix(INV, 1), S1 = P::stride(INV, 1);
         pass_store<N, R0, S0>(v, sm, t);
         __syncthreads();
         pass_load<N, R1>(v, sm, t);
         __syncthreads();
-        pass_compute<N, R1, S1, DIR>(v, t, tw);
+        pass_compute<N, R1, S1, DIR>(v, t, tw + P::tw_offset(INV, 1));
         if constexpr (P::NP > 2) {
             constexpr int R2 = P::radix(INV, 2), S2 = P::stride(INV, 2);
             pass_store<N, R1, S1>(v, sm, t);
             __syncthreads();
             pass_load<N, R2>(v, sm, t);
             __syncthreads();
-            pass_compute<N, R2, S2, DIR>(v, t, tw);
+            pass_compute<N, R2, S2, DIR>(v, t, tw + P::tw_offset(INV, 2));
             if constexpr (P::NP > 3) {
                 constexpr int R3 = P::radix(INV, 3), S3 = P::stride(INV, 3);
                 pass_store<N, R2, S2>(v, sm, t);
                 __syncthreads();
                 pass_load<N, R3>(v, sm, t);
                 __syncthreads();
-                pass_compute<N, R3, S3, DIR>(v, t, tw);
+                pass_compute<N, R3, S3, DIR>(v, t, tw + P::tw_offset(INV, 3));
             }
         }
     }

@@ -1,4 +1,6 @@
 // Launchers of the fused 2D engine: runtime grid size -> compile-time kernel instantiation.
+#include <cmath>
+
 #include "fused2d.h"
 #include "fused2d.cuh"
 
@@ -10,14 +12,15 @@ namespace {
 template <typename T, int N>
 cudaError_t attrs() {
     using F = Fused2D<N>;
-    const int row_smem = (int)RowPairs<N>::smem_bytes(sizeof(Pair<T>));
+    const int row_smem = (int)RowSingle<N>::smem_bytes(sizeof(cplx<T>));
+    const int max_smem = (int)RowPairs<N>::smem_bytes(sizeof(Pair<T>));
     const int col_smem = (int)F::template smem_bytes<Pair<T>>();
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(k_row_pass<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   row_smem)))
         return e;
     if ((e = cudaFuncSetAttribute(k_row_max<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  row_smem)))
+                                  max_smem)))
         return e;
     if ((e = cudaFuncSetAttribute(k_col_pass<T, N, -1>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
@@ -37,8 +40,8 @@ cudaError_t attrs() {
 
 template <typename T, int N>
 cudaError_t row(void* X, int kc, const void* tw, cudaStream_t st) {
-    using F = RowPairs<N>;
-    k_row_pass<T, N><<<(N / 2) / F::B, F::THREADS, F::smem_bytes(sizeof(Pair<T>)), st>>>(
+    using F = RowSingle<N>;
+    k_row_pass<T, N><<<N / F::B, F::THREADS, F::smem_bytes(sizeof(cplx<T>)), st>>>(
         (Pair<T>*)X, kc, (const cplx<T>*)tw);
     return cudaGetLastError();
 }
@@ -108,7 +111,53 @@ cudaError_t dispatch(int n, int fp64, Fn&& fn) {
     }
 }
 
+template <int N>
+void fill_table(double* out) {
+    using P = FftPlan<N>;
+    for (int dir = 0; dir < 2; ++dir) {
+        const bool inv = dir == 0;
+        for (int p = 1; p < P::NP; ++p) {
+            const int S = P::stride(inv, p), R = P::radix(inv, p), o = P::tw_offset(inv, p);
+            for (int js = 0; js < S; ++js) {
+                const double a = 2.0 * M_PI * (double)js / (double)(S * R);
+                const int q[3] = {1, 4, 8};
+                for (int r = 0; r < 3; ++r) {
+                    out[2 * (o + r * S + js)] = std::cos(q[r] * a);
+                    out[2 * (o + r * S + js) + 1] = std::sin(q[r] * a);
+                }
+            }
+        }
+    }
+}
+
+template <typename Fn>
+auto by_size(int n, Fn&& fn) {
+    switch (n) {
+        case 16: return fn.template operator()<16>();
+        case 32: return fn.template operator()<32>();
+        case 64: return fn.template operator()<64>();
+        case 128: return fn.template operator()<128>();
+        case 256: return fn.template operator()<256>();
+        case 512: return fn.template operator()<512>();
+        case 1024: return fn.template operator()<1024>();
+        case 2048: return fn.template operator()<2048>();
+        case 4096: return fn.template operator()<4096>();
+        default: return fn.template operator()<8192>();
+    }
+}
+
 }  // namespace
+
+int twiddle_table_size(int n) {
+    return by_size(n, []<int N>() { return FftPlan<N>::TW_SIZE; });
+}
+
+void fill_twiddles(int n, double* out) {
+    by_size(n, [&]<int N>() {
+        fill_table<N>(out);
+        return 0;
+    });
+}
 
 bool supported(int n, int fp64) {
     if (n < 16 || (n & (n - 1))) return false;

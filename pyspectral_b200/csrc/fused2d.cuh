@@ -8,7 +8,7 @@
 // pairs, X[x/2][ky][x%2] (xidx): a column access then moves whole 32-byte sectors (rows x and
 // x+1 of one column are adjacent) and a row-pair access is contiguous.
 //
-// Row pass (one CTA sub-block per row pair, both rows transformed together as a Pair):
+// Row pass (one CTA sub-block per row; two CTAs per SM):
 //   Z(k) = U(k) + i V(k) (Hermitian completion of both half spectra), z = IFFT_n(Z) gives
 //   z = u + i v; the products (v^2 - u^2) + i (u v) are formed in registers; Z' = FFT_n of
 //   that; P(k) = (Z'(k) + conj Z'(n-k)) / 2, Q(k) = (Z'(k) - conj Z'(n-k)) / 2i for k < kc.
@@ -67,37 +67,43 @@ struct RowPairs {
     static constexpr size_t smem_bytes(size_t elem) { return (size_t)B * FftPlan<N>::SMEM * elem; }
 };
 
+// Rows per CTA for the row pass: single-row sub-blocks, at least 256 threads per CTA, two CTAs
+// resident per SM (64 registers per thread at 512 threads).
+template <int N>
+struct RowSingle {
+    static constexpr int T = N / 16;
+    static constexpr int B = T >= 256 ? 1 : (256 / T < N ? 256 / T : N);
+    static constexpr int THREADS = T * B;
+    static constexpr size_t smem_bytes(size_t elem) { return (size_t)B * FftPlan<N>::SMEM * elem; }
+};
+
 template <typename T, int N>
-__global__ void __launch_bounds__(RowPairs<N>::THREADS) k_row_pass(Pair<T>* __restrict__ X,
-                                                                  int kc,
-                                                                  const cplx<T>* __restrict__ tw) {
-    using F = RowPairs<N>;
+__global__ void __launch_bounds__(RowSingle<N>::THREADS, 2) k_row_pass(Pair<T>* __restrict__ X,
+                                                                      int kc,
+                                                                      const cplx<T>* __restrict__ tw) {
+    using F = RowSingle<N>;
     constexpr int TT = F::T;
     constexpr int RI = first_radix<N, true>();   // inverse input pattern
     constexpr int RF = last_radix<N, false>();   // forward output pattern
     static_assert(last_radix<N, true>() == first_radix<N, false>(), "register hand-off");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int sub = threadIdx.x / TT, t = threadIdx.x % TT;
-    Pair<T>* sm = reinterpret_cast<Pair<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
-    const int p = blockIdx.x * F::B + sub;  // row pair: rows 2p (.a) and 2p + 1 (.b)
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
+    const int row = blockIdx.x * F::B + sub;  // n is a multiple of B
+    const int p = row >> 1, half = row & 1;
 
-    Pair<T> v[16];
+    cplx<T> v[16];
 #pragma unroll
     for (int g = 0; g < 16 / RI; ++g)
 #pragma unroll
-        for (int m = 0; m < RI; ++m) {
-            const int k = in_pos<N, RI>(t, g, m);
-            v[g * RI + m] = Pair<T>{row_input<T, N>(X, p, k, kc, 0), row_input<T, N>(X, p, k, kc, 1)};
-        }
+        for (int m = 0; m < RI; ++m)
+            v[g * RI + m] = row_input<T, N>(X, p, in_pos<N, RI>(t, g, m), kc, half);
     block_fft<N, true>(v, sm, t, tw);
-    // physical space, each row: z = u + i v  ->  (v^2 - u^2) + i (u v)
+    // physical space: z = u + i v  ->  (v^2 - u^2) + i (u v)
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
-        T u = v[e].a.x, w = v[e].a.y;
-        v[e].a = mk<T>((w - u) * (w + u), u * w);
-        u = v[e].b.x;
-        w = v[e].b.y;
-        v[e].b = mk<T>((w - u) * (w + u), u * w);
+        T u = v[e].x, w = v[e].y;
+        v[e] = mk<T>((w - u) * (w + u), u * w);
     }
     __syncthreads();
     block_fft<N, false>(v, sm, t, tw);
@@ -107,17 +113,13 @@ __global__ void __launch_bounds__(RowPairs<N>::THREADS) k_row_pass(Pair<T>* __re
 #pragma unroll
         for (int m = 0; m < RF; ++m) sm[spad(in_pos<N, RF>(t, g, m))] = v[g * RF + m];
     __syncthreads();
-    // P(k) = (Z'(k) + conj Z'(n-k)) / 2, Q(k) = (Z'(k) - conj Z'(n-k)) / 2i, for each row
+    // P(k) = (Z'(k) + conj Z'(n-k)) / 2, Q(k) = (Z'(k) - conj Z'(n-k)) / 2i
     for (int k = t; k < kc; k += TT) {
-        Pair<T> a = sm[spad(k)], b = sm[spad((N - k) & (N - 1))];
-        Pair<T> o0, o1;
-        o0.a = mk<T>((T)0.5 * (a.a.x + b.a.x), (T)0.5 * (a.a.y - b.a.y));
-        o0.b = mk<T>((T)0.5 * (a.a.y + b.a.y), (T)0.5 * (b.a.x - a.a.x));
-        o1.a = mk<T>((T)0.5 * (a.b.x + b.b.x), (T)0.5 * (a.b.y - b.b.y));
-        o1.b = mk<T>((T)0.5 * (a.b.y + b.b.y), (T)0.5 * (b.b.x - a.b.x));
-        Pair<T>* dst = X + ((size_t)p * kc + k) * 2;
-        dst[0] = o0;
-        dst[1] = o1;
+        cplx<T> a = sm[spad(k)], b = sm[spad((N - k) & (N - 1))];
+        Pair<T> o;
+        o.a = mk<T>((T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y));
+        o.b = mk<T>((T)0.5 * (a.y + b.y), (T)0.5 * (b.x - a.x));
+        X[((size_t)p * kc + k) * 2 + half] = o;
     }
 }
 

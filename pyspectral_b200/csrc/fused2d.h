@@ -14,6 +14,10 @@ bool supported(int n, int fp64);
 inline int kc_of(int n) { return (n + 2) / 3; }
 // Opt every kernel of this size into its dynamic shared memory; once per process and size.
 cudaError_t set_attributes(int n, int fp64);
+// Complex entries of the per-pass twiddle table of a length-n transform, and the table itself
+// (fp64, interleaved re/im, 2 * twiddle_table_size(n) doubles).
+int twiddle_table_size(int n);
+void fill_twiddles(int n, double* out);
 
 cudaError_t row_pass(int n, int fp64, void* X, int kc, const void* tw, cudaStream_t st);
 cudaError_t row_max(int n, int fp64, const void* X, int kc, const void* tw,

@@ -446,7 +446,9 @@ sp_solver* sp_create(int n, int dim, int form, int fp64, int fft_mode, int* stat
     s->off_umax = off; off += align256(4 * sizeof(unsigned long long));
     s->off_out = off; off += align256(8 * sizeof(double));
     s->off_spec = off; off += align256((size_t)s->nshell * sizeof(double));
-    s->off_tw = off; off += align256((size_t)n * 2 * s->rsize);
+    s->off_tw = off;
+    if (fft_mode == SP_FFT_FUSED && sp::fused::supported(n, fp64))
+        off += align256((size_t)sp::fused::twiddle_table_size(n) * 2 * s->rsize);
     s->aux_bytes = off;
     s->work_bytes = (size_t)s->nwork * field_bytes(s);
 
@@ -532,13 +534,9 @@ int sp_bind(sp_solver* s, void* u0, void* acc, void* work, void* aux, void* fft_
     s->params_valid = false;
     drop_graph(s);
     if (s->fused()) {
-        // twiddle table tw[i] = exp(+2 pi i i / n), fp64 on the host, rounded to the real type
-        std::vector<double> tw(2 * (size_t)s->n);
-        for (int i = 0; i < s->n; ++i) {
-            double a = 2.0 * M_PI * (double)i / (double)s->n;
-            tw[2 * i] = std::cos(a);
-            tw[2 * i + 1] = std::sin(a);
-        }
+        // per-pass twiddle table, fp64 on the host, rounded to the real type
+        std::vector<double> tw(2 * (size_t)sp::fused::twiddle_table_size(s->n));
+        sp::fused::fill_twiddles(s->n, tw.data());
         if (s->fp64) {
             SP_CUDA(cudaMemcpy(s->tw_dev(), tw.data(), tw.size() * sizeof(double),
                                cudaMemcpyHostToDevice));
