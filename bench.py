@@ -443,12 +443,19 @@ def main(argv: list[str] | None = None) -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="decay2d-8192-fp32", choices=sorted(WORKLOADS))
-    ap.add_argument("--variant", default="b200/fused-inplace-graph")
+    ap.add_argument("--variant", default="auto",
+                    help="registry variant; auto = the fused-FFT engine where it runs (2D, n a "
+                         "power of two <= 8192 fp32 / 4096 fp64), else the cuFFT graph engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
     if args.impl == "ours":
         args.warmup = max(args.warmup, 3)  # at least 3 untimed warm-up steps
     w = WORKLOADS[args.workload]
+    if args.variant == "auto":
+        n = w["n"]
+        fused_ok = (w["dim"] == 2 and n & (n - 1) == 0 and 16 <= n
+                    and n <= (8192 if w["dtype"] == "float32" else 4096))
+        args.variant = "b200/fused-fft-graph" if fused_ok else "b200/fused-inplace-graph"
     if args.impl == "reference":
         return reference_arm(args, w)
     return ours(args, w)

@@ -210,17 +210,19 @@ struct FftPlan {
         return s;
     }
     // Per-pass twiddle table: for the inverse passes p = 1..NP-1, then the forward passes
-    // p = 1..NP-1, a block of 3 S_p entries [w^1 | w^4 | w^8], w = exp(+2 pi i js / (S_p R_p)),
-    // js < S_p.  tw_offset is the start of a pass's block; TW_SIZE the whole table.
+    // p = 1..NP-1, a block of npow(R_p) S_p entries: the stored powers w^q (q = 1, 2, 3, 4, 8,
+    // 12, the first npow of them) of w = exp(+2 pi i js / (S_p R_p)), js < S_p, laid out
+    // [power][js].  tw_offset is the start of a pass's block; TW_SIZE the whole table.
+    static constexpr int npow(int r) { return r == 2 ? 1 : r == 4 ? 3 : r == 8 ? 4 : 6; }
     static constexpr int tw_offset(bool inv, int p) {
         int o = 0;
         for (int q = 1; q < NP; ++q) {
             if (inv && q == p) return o;
-            o += 3 * stride(true, q);
+            o += npow(radix(true, q)) * stride(true, q);
         }
         for (int q = 1; q < NP; ++q) {
             if (!inv && q == p) return o;
-            o += 3 * stride(false, q);
+            o += npow(radix(false, q)) * stride(false, q);
         }
         return o;
     }
@@ -243,29 +245,33 @@ __device__ __forceinline__ C tw_load(const C* __restrict__ tw, int idx) {
     return w;
 }
 
-// Twiddles w^m, m = 1..R-1, of one group: three table loads (w, w^4, w^8) and at most three
-// dependent complex products for the others, instead of R-1 scattered table loads.  `tw`
-// points at this pass's block [w^1 | w^4 | w^8] x S of the per-pass table, so the loads of a
-// warp (consecutive js) are contiguous.
+// Powers of w stored per pass (see FftPlan::tw_offset): w^1, w^2, w^3 (radix >= 4), w^4
+// (radix >= 8), w^8 and w^12 (radix 16).  Every other power is one product of two stored,
+// correctly rounded values, so each twiddle is within about one rounding of exact.
+template <int R>
+constexpr int tw_powers() { return R == 2 ? 1 : R == 4 ? 3 : R == 8 ? 4 : 6; }
+
+// Twiddles w^m, m = 1..R-1, of one group from this pass's block, laid out [power][js]: a warp
+// (consecutive js) reads each stored power contiguously.
 template <int R, int S, int DIR, typename C>
 __device__ __forceinline__ void group_twiddles(C (&w)[16], const C* __restrict__ tw, int js) {
     w[1] = tw_load<DIR>(tw, js);
     if constexpr (R >= 4) {
-        w[2] = cmul(w[1], w[1]);
-        w[3] = cmul(w[2], w[1]);
+        w[2] = tw_load<DIR>(tw, S + js);
+        w[3] = tw_load<DIR>(tw, 2 * S + js);
     }
     if constexpr (R >= 8) {
-        w[4] = tw_load<DIR>(tw, S + js);
+        w[4] = tw_load<DIR>(tw, 3 * S + js);
         w[5] = cmul(w[4], w[1]);
         w[6] = cmul(w[4], w[2]);
         w[7] = cmul(w[4], w[3]);
     }
     if constexpr (R >= 16) {
-        w[8] = tw_load<DIR>(tw, 2 * S + js);
+        w[8] = tw_load<DIR>(tw, 4 * S + js);
+        w[12] = tw_load<DIR>(tw, 5 * S + js);
         w[9] = cmul(w[8], w[1]);
         w[10] = cmul(w[8], w[2]);
         w[11] = cmul(w[8], w[3]);
-        w[12] = cmul(w[8], w[4]);
         w[13] = cmul(w[12], w[1]);
         w[14] = cmul(w[12], w[2]);
         w[15] = cmul(w[12], w[3]);

@@ -118,14 +118,15 @@ void fill_table(double* out) {
         const bool inv = dir == 0;
         for (int p = 1; p < P::NP; ++p) {
             const int S = P::stride(inv, p), R = P::radix(inv, p), o = P::tw_offset(inv, p);
-            for (int js = 0; js < S; ++js) {
-                const double a = 2.0 * M_PI * (double)js / (double)(S * R);
-                const int q[3] = {1, 4, 8};
-                for (int r = 0; r < 3; ++r) {
-                    out[2 * (o + r * S + js)] = std::cos(q[r] * a);
-                    out[2 * (o + r * S + js) + 1] = std::sin(q[r] * a);
+            const int pw[6] = {1, 2, 3, 4, 8, 12};
+            for (int k = 0; k < P::npow(R); ++k)
+                for (int js = 0; js < S; ++js) {
+                    // exp(+2 pi i js q / (S R)); reduce the exponent first for an exact angle
+                    const long e = ((long)js * pw[k]) % (S * R);
+                    const double a = 2.0 * M_PI * (double)e / (double)(S * R);
+                    out[2 * (o + k * S + js)] = std::cos(a);
+                    out[2 * (o + k * S + js) + 1] = std::sin(a);
                 }
-            }
         }
     }
 }
