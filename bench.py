@@ -64,6 +64,50 @@ def dist_env() -> tuple[int, int, int]:
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
+class Replicas:
+    """Plumbing of ``--gpus N``: one process per GPU, each running its own replica of the
+    workload (the step does not shard).  The only collectives are a barrier around the timed
+    region and the max of the per-rank times; ``nccl`` on the GPU box, ``gloo`` in CPU tests."""
+
+    def __init__(self, backend: str = "nccl", device: object = None) -> None:
+        self.rank, self.world, self.local = dist_env()
+        self.pg = None
+        self.device = device
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            kw = {"device_id": device} if backend == "nccl" and device is not None else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300), **kw)
+            self.pg = dist
+
+    def barrier(self) -> None:
+        if self.pg is not None:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        """Max of a float over all ranks (every rank calls it, in the same order)."""
+        if self.pg is None:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64,
+                         device=self.device if self.device is not None else "cpu")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self) -> None:
+        if self.pg is not None:
+            self.pg.destroy_process_group()
+            self.pg = None
+
+
+def aggregate_mpts(world: int, points_per_replica: float, seconds_per_step: float) -> float:
+    """Whole-job throughput: every replica advances its own grid in the (max) step time."""
+    return world * points_per_replica / seconds_per_step / 1e6
+
+
 def make_config(w: dict):
     from pyspectral_b200 import Config
 
@@ -257,26 +301,8 @@ def ours(args, w: dict) -> int:
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-        pg = dist
-
-    def barrier() -> None:
-        if pg is not None:
-            pg.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if pg is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    comm = Replicas("nccl", torch.device("cuda", local))
+    barrier, max_over_ranks = comm.barrier, comm.max
 
     from pyspectral_b200.registry import make_solver
 
@@ -306,7 +332,7 @@ def ours(args, w: dict) -> int:
     t_ms = max_over_ranks(ev0.elapsed_time(ev1))
     ms_step = t_ms / args.steps
     npts = float(w["n"]) ** w["dim"]
-    value = world * npts / (ms_step * 1e-3) / 1e6
+    value = aggregate_mpts(world, npts, ms_step * 1e-3)
 
     # ---- end to end through the public API: host state in, K steps, host state out
     s2 = make_solver(args.variant, cfg)
@@ -431,8 +457,7 @@ def ours(args, w: dict) -> int:
                       f"pyspectral NumpySolver, scipy.fft workers=-1"}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if pg is not None:
-        pg.destroy_process_group()
+    comm.close()
     return 0
 
 

@@ -391,3 +391,31 @@ def test_fused_rejects_what_it_does_not_run():
     for cfg in (Config(n=48, dim=2), Config(n=16, dim=3), Config(n=8192, dim=2, dtype="float64")):
         with pytest.raises(BackendUnavailable):
             get(FUSED).make(cfg)
+
+
+def test_fused_checkpoint_resume_is_bit_identical(tmp_path):
+    from pyspectral_b200.checkpoint import load_checkpoint, save_checkpoint
+    from pyspectral_b200.simulate import run
+
+    cfg = Config(n=512, dim=2, nu=1e-4, dtype="float32", force_klo=3, force_khi=5)
+    ic = initial.random_phase_2d(512, k0=10, seed=7)
+    whole = get(FUSED).make(cfg)
+    whole.set_state(ic)
+    run(whole, 0.02, dt=1e-3, target_power=1e-3)
+    a = get(FUSED).make(cfg)
+    a.set_state(ic)
+    res = run(a, 0.01, dt=1e-3, target_power=1e-3)
+    ck = save_checkpoint(tmp_path / "ck.npz", a, res)
+    b = get(FUSED).make(cfg)
+    prev, _ = load_checkpoint(ck, b)
+    run(b, 0.02, dt=1e-3, target_power=1e-3, result=prev)
+    assert np.array_equal(b.get_state(), whole.get_state())
+
+
+def test_cli_run_on_device(tmp_path, capsys):
+    from pyspectral_b200.cli import main
+
+    out = tmp_path / "ck.npz"
+    assert main(["run", "--backend", FUSED, "--n", "64", "--t-end", "0.1", "--case", "tgv",
+                 "--dtype", "float64", "--out", str(out)]) == 0
+    assert "steps" in capsys.readouterr().out and out.exists()

@@ -155,6 +155,17 @@ class _OracleAsSolver:
         self.amps.append(a)
         self._s.set_forcing_amplitude(a)
 
+    @property
+    def force_amp(self):
+        return self._s.force_amp
+
+    @t.setter
+    def t(self, value):
+        self._s.t = value
+
+    def get_state(self):
+        return self._s.get_state()
+
     def synchronize(self):
         pass
 
@@ -247,3 +258,36 @@ def test_plugin_class_raises_pyspectral_unavailable():
     cls = _plugin_class("B200Solver")
     with pytest.raises(RefUnavailable):
         cls(RefConfig(n=16, dim=2, form="advective"))
+
+
+# ----------------------------------------------------------------------------- checkpoint / CLI
+def test_checkpoint_roundtrip_and_chunked_resume(tmp_path):
+    from pyspectral_b200.checkpoint import load_checkpoint, save_checkpoint
+
+    cfg = Config(n=16, dim=2, nu=0.01, force_klo=1, force_khi=2.5, dtype="float32")
+    ic = initial.to_spectral(initial.random_2d(16, k0=3), 2)
+    whole = _OracleAsSolver(cfg)
+    whole.set_state(ic)
+    run(whole, 0.2, dt=0.01, diag_dt=0.05)
+    # same run in two chunks through a checkpoint
+    a = _OracleAsSolver(cfg)
+    a.set_state(ic)
+    res = run(a, 0.1, dt=0.01, diag_dt=0.05)
+    a.set_forcing_amplitude(0.0)
+    ck = save_checkpoint(tmp_path / "ck.npz", a, res)
+    z = np.load(ck)
+    assert z["state"].dtype == np.complex64 and float(z["t"]) == pytest.approx(0.1)
+    b = _OracleAsSolver(cfg)
+    prev, _ = load_checkpoint(ck, b)
+    assert b.t == pytest.approx(0.1) and prev.t == res.t
+    res2 = run(b, 0.2, dt=0.01, diag_dt=0.05, result=prev)
+    assert res2.t[-1] == pytest.approx(0.2)
+    np.testing.assert_allclose(b.get_state(), whole.get_state(), rtol=0, atol=1e-5)
+
+
+def test_cli_list_reports_every_variant(capsys):
+    from pyspectral_b200.cli import main
+
+    assert main(["list"]) == 0
+    out = capsys.readouterr().out
+    assert "b200/fused-fft-graph" in out and "b200/fused-inplace-graph" in out
