@@ -26,11 +26,18 @@
 
 namespace sp {
 
-// sub-blocks (rows or columns) per CTA: at least 256 threads per CTA, at most N sub-blocks
+// Sub-blocks (columns) per CTA: one sequence per CTA once a sequence has at least 16 threads
+// (n >= 256), so small grids still spread over every SM; smaller n packs sequences into one
+// warp.  Never more sub-blocks than sequences.
+constexpr int sub_blocks(int t, int count) {
+    const int b = t >= 16 ? 1 : 32 / t;
+    return b < count ? b : count;
+}
+
 template <int N>
 struct Fused2D {
     static constexpr int T = N / 16;
-    static constexpr int B = T >= 256 ? 1 : (256 / T < N ? 256 / T : N);
+    static constexpr int B = sub_blocks(T, N);
     static constexpr int THREADS = T * B;
     template <typename E>
     static constexpr size_t smem_bytes() { return (size_t)B * FftPlan<N>::SMEM * sizeof(E); }
@@ -62,17 +69,17 @@ __device__ __forceinline__ cplx<T> row_input(const Pair<T>* __restrict__ X, int 
 template <int N>
 struct RowPairs {
     static constexpr int T = N / 16;
-    static constexpr int B = T >= 256 ? 1 : (256 / T < N / 2 ? 256 / T : N / 2);
+    static constexpr int B = sub_blocks(T, N / 2);
     static constexpr int THREADS = T * B;
     static constexpr size_t smem_bytes(size_t elem) { return (size_t)B * FftPlan<N>::SMEM * elem; }
 };
 
-// Rows per CTA for the row pass: single-row sub-blocks, at least 256 threads per CTA, two CTAs
-// resident per SM (64 registers per thread at 512 threads).
+// Rows per CTA for the row pass: single-row sub-blocks (see sub_blocks), two CTAs resident
+// per SM at n = 8192 (64 registers per thread at 512 threads).
 template <int N>
 struct RowSingle {
     static constexpr int T = N / 16;
-    static constexpr int B = T >= 256 ? 1 : (256 / T < N ? 256 / T : N);
+    static constexpr int B = sub_blocks(T, N);
     static constexpr int THREADS = T * B;
     static constexpr size_t smem_bytes(size_t elem) { return (size_t)B * FftPlan<N>::SMEM * elem; }
 };
