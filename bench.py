@@ -53,6 +53,10 @@ WORKLOADS = {
                                       form="rotational", ic="tgv3d", cfl=0.5),
     "tgv3d-512-fp32-basdevant": dict(n=512, dim=3, dtype="float32", nu=1 / 1600,
                                      form="basdevant", ic="tgv3d", cfl=0.5),
+    # 256 forced runs of uneven size advanced together: 64 each at 128^2 .. 1024^2, fp32
+    "ensemble-4x64-fp32": dict(ensemble=True, sizes=(128, 256, 512, 1024), per_size=64,
+                               dtype="float32", dim=2, form="basdevant", k0=8.0, power=1e-3,
+                               klo=10.0, khi=12.0, alpha=0.1, alpha_kmax=2.0, cfl=0.5),
 }
 PUBLISHED_MPTS = {"decay2d-8192-fp32": 547.0}  # reference, RTX 3070 Laptop, fused-inplace
 FALLBACK_HBM_GBS = 6650.0
@@ -243,6 +247,158 @@ def run_workload(s, w: dict, nsteps: int) -> None:
         s.advance(nsteps, w["dt"])
     else:
         run_steps(s, nsteps, cfl=w["cfl"], dt_max=0.05, cfl_every=10)
+
+
+# ----------------------------------------------------------------------------- ensemble
+def ensemble_members(w: dict) -> list:
+    """The ensemble workload: run i (seed i) of each size class, nu from k_max eta = 1."""
+    from pyspectral_b200 import Config
+    from pyspectral_b200.ensemble import nu_for_kmax_eta
+
+    kf = 0.5 * (w["klo"] + w["khi"])
+    out = []
+    for n in w["sizes"]:
+        for _ in range(w["per_size"]):
+            out.append(Config(n=n, dim=2, nu=nu_for_kmax_eta(n, w["power"], kf),
+                              alpha=w["alpha"], alpha_kmax=w["alpha_kmax"],
+                              force_klo=w["klo"], force_khi=w["khi"], dtype=w["dtype"]))
+    return out
+
+
+def ensemble_ics(w: dict, members: list) -> list:
+    from pyspectral_b200 import initial
+
+    return [initial.random_phase_2d(c.n, k0=w["k0"], seed=i % w["per_size"], energy=0.5)
+            for i, c in enumerate(members)]
+
+
+def time_oracle_ensemble(w: dict) -> dict:
+    """One member per size class on the host (oracle port), scaled to the whole ensemble."""
+    from oracle.numpy_oracle import OracleSolver
+    from pyspectral_b200.ensemble import nu_for_kmax_eta
+
+    total_s, pts = 0.0, 0.0
+    kf = 0.5 * (w["klo"] + w["khi"])
+    for n in w["sizes"]:
+        from pyspectral_b200 import initial
+
+        s = OracleSolver(n, 2, nu=nu_for_kmax_eta(n, w["power"], kf), alpha=w["alpha"],
+                         alpha_kmax=w["alpha_kmax"], force_amp=0.1, force_klo=w["klo"],
+                         force_khi=w["khi"], dtype=w["dtype"])
+        s.set_state(initial.random_phase_2d(n, k0=w["k0"], seed=0))
+        s.step(1e-4)
+        t0 = time.perf_counter()
+        for _ in range(2):
+            s.step(1e-4)
+        total_s += w["per_size"] * (time.perf_counter() - t0) / 2
+        pts += w["per_size"] * float(n) ** 2
+    return {"sec_per_step": total_s, "mpts": pts / total_s / 1e6, "cores": os.cpu_count() or 1}
+
+
+def ensemble_fft_stage_ms(w: dict) -> float:
+    """Standalone batched cuFFT time of one RK stage for every class (2 C2R + 2 R2C per member,
+    batched over the class, through torch.fft), summed over the classes."""
+    import torch
+
+    cdt = torch.complex64 if w["dtype"] == "float32" else torch.complex128
+    rdt = torch.float32 if w["dtype"] == "float32" else torch.float64
+    tot = 0.0
+    for n in w["sizes"]:
+        b = 2 * w["per_size"]
+        q = torch.zeros((b, n, n // 2 + 1), dtype=cdt, device="cuda")
+        r = torch.zeros((b, n, n), dtype=rdt, device="cuda")
+
+        def stage() -> None:
+            torch.fft.irfftn(q, s=(n, n), dim=(-2, -1), out=r)
+            torch.fft.rfftn(r, dim=(-2, -1), out=q)
+
+        for _ in range(3):
+            stage()
+        tot += event_time_ms(stage, 10)
+        del q, r
+    torch.cuda.empty_cache()
+    return tot
+
+
+def ours_ensemble(args, w: dict) -> int:
+    import torch
+
+    from pyspectral_b200.ensemble import Ensemble
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    comm = Replicas("nccl", torch.device("cuda", local))
+    members = ensemble_members(w)
+    ics = ensemble_ics(w, members)
+    ens = Ensemble(members)
+    ens.set_states(ics)
+    ens.run_steps(args.warmup, cfl=w["cfl"], target_power=w["power"])
+    torch.cuda.synchronize()
+    comm.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = ens.kernel_launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    ens.run_steps(args.steps, cfl=w["cfl"], target_power=w["power"])
+    ev1.record()
+    ev1.synchronize()
+    comm.barrier()
+    clk = clocks.stop()
+    launches = ens.kernel_launches - l0
+    ms_step = comm.max(ev0.elapsed_time(ev1)) / args.steps
+    pts = sum(float(c.n) ** 2 for c in members)
+    value = aggregate_mpts(world, pts, ms_step * 1e-3)
+    # end to end: host states in, K steps, host states out
+    e2 = Ensemble(members)
+    e2.set_states(ics)
+    torch.cuda.synchronize()
+    comm.barrier()
+    t0 = time.perf_counter()
+    e2.set_states(ics)
+    e2.run_steps(args.steps, cfl=w["cfl"], target_power=w["power"])
+    outs = [e2.get_state(i) for i in range(len(members))]
+    e2e_s = comm.max(time.perf_counter() - t0)
+    state_bytes = sum(c.u0.nbytes for c in e2.classes)
+    del e2, outs
+    torch.cuda.empty_cache()
+    # aggregate FFT roofline of the reference's definition, summed over the classes
+    t_fft_stage = ensemble_fft_stage_ms(w)
+    bcopy = copy_bandwidth_gbs()
+    pw = sum(w["per_size"] * traffic_model(n, 2, "basdevant", w["dtype"])["pointwise_bytes"]
+             for n in w["sizes"])
+    t_roof = 4 * t_fft_stage + pw / (bcopy * 1e9) * 1e3
+    line = {
+        "metric": "Mpts/s/RK4 step", "value": value, "unit": "Mpts/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if w["dtype"] == "float32" else "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "sizes": list(w["sizes"]),
+                   "runs_per_size": w["per_size"], "members": len(members),
+                   "forcing": f"constant power P={w['power']} on {w['klo']}<=|k|<={w['khi']}",
+                   "drag": f"alpha={w['alpha']} on |k|<={w['alpha_kmax']}",
+                   "nu": "k_max eta = 1 (nu_for_kmax_eta)", "cfl": w["cfl"],
+                   "engine": "sp_batch per size class, one sp_group graph",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "pct_fft_roofline": 100.0 * t_roof / ms_step,
+        "fft_roofline": {"t_fft_stage_ms_all_classes": t_fft_stage, "t_roofline_step_ms": t_roof,
+                         "copy_bw_gbs": bcopy, "pointwise_bytes": pw},
+        "e2e": {"value": aggregate_mpts(world, pts * args.steps, e2e_s), "unit": "Mpts/s",
+                "h2d_bytes_per_step": state_bytes / args.steps,
+                "d2h_bytes_per_step": state_bytes / args.steps,
+                "what": "set_states(host) + K steps + get_state of every member, wall clock"},
+        "gpu_launches": launches, "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = time_oracle_ensemble(w)
+        line["cpu_baseline"] = {"value": r["mpts"], "unit": "Mpts/s", "cores": r["cores"],
+                                "kind": "port",
+                                "sample": "2 IF-RK4 steps of one member per size class (oracle "
+                                          "port, scipy.fft workers=-1), times 64 members"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    comm.close()
+    return 0
 
 
 # ----------------------------------------------------------------------------- CPU side
@@ -476,6 +632,24 @@ def main(argv: list[str] | None = None) -> int:
     if args.impl == "ours":
         args.warmup = max(args.warmup, 3)  # at least 3 untimed warm-up steps
     w = WORKLOADS[args.workload]
+    if w.get("ensemble"):
+        if args.impl == "reference":
+            rank, _, _ = dist_env()
+            if rank != 0:
+                return 0
+            r = time_oracle_ensemble(w)
+            print(json.dumps({
+                "metric": "Mpts/s/RK4 step", "value": r["mpts"], "unit": "Mpts/s",
+                "impl": "reference", "n_gpus": 1, "steps": 2, "warmup": 1,
+                "ms_per_step": r["sec_per_step"] * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": args.workload},
+                "cpu_baseline": {"value": r["mpts"], "unit": "Mpts/s", "cores": r["cores"],
+                                 "kind": "port", "sample": "one member per class, x64"},
+                "e2e": {"value": r["mpts"], "unit": "Mpts/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}), flush=True)
+            return 0
+        return ours_ensemble(args, w)
     if args.variant == "auto":
         n = w["n"]
         fused_ok = (w["dim"] == 2 and n & (n - 1) == 0 and 16 <= n

@@ -172,6 +172,45 @@ const char* sp_last_error(const sp_solver* s);
 /* Message of the last sp_create (or sp_spectrum_noalloc) failure in this thread (never NULL). */
 const char* sp_create_error(void);
 
+/* ---------------------------------------------------------------- batched ensembles
+ * No counterpart in the reference (one pyspectral solver is one run).  A batch advances
+ * `members` independent 2D runs of one grid size on the fused-FFT engine, one launch per phase
+ * for all members, each member with its own viscosity, time step and forcing amplitude; a
+ * group steps several batches (uneven sizes) from one CUDA graph. */
+typedef struct sp_batch sp_batch;
+typedef struct sp_group sp_group;
+
+/* n a power of two, 16..8192 (fp32) / 16..4096 (fp64); members 1..65535. */
+sp_batch* sp_batch_create(int n, int fp64, int members, int* status);
+void sp_batch_destroy(sp_batch* b);
+/* out = [members, kc, state bytes (u0: members x n x (n/2+1) complex, NumPy layout each),
+ *        0, work bytes, aux bytes] (count <= 6). */
+int sp_batch_query_sizes(const sp_batch* b, int64_t* out, int count);
+int sp_batch_bind(sp_batch* b, void* u0, void* work, void* aux);
+/* nu: one viscosity per member; drag alpha on k^2 <= drag_k2; forcing band [klo, khi]. */
+int sp_batch_set_physics(sp_batch* b, const double* nu, double alpha, double drag_k2,
+                         double force_klo, double force_khi);
+/* Per-member time step and band-forcing rate (host arrays, `amp` may be NULL); uploaded on
+ * `stream` when they change; used by the following steps. */
+int sp_batch_set_step(sp_batch* b, const double* dt, const double* amp, void* stream);
+/* Load the states written into u0 (dealias, transpose, stage-0 inputs). */
+int sp_batch_prepare(sp_batch* b, void* stream);
+int sp_batch_step(sp_batch* b, void* stream);
+/* Write the members' states back into u0 (NumPy layout) when they changed. */
+int sp_batch_sync_state(sp_batch* b, void* stream);
+/* out[m * 4 + q]: energy, enstrophy, palinstrophy, energy in band_klo <= |k| <= band_khi. */
+int sp_batch_diagnostics(sp_batch* b, double band_klo, double band_khi, double* out,
+                         void* stream);
+/* out[m] = max|u| + max|v| of member m (CFL). */
+int sp_batch_max_velocity(sp_batch* b, double* out, void* stream);
+int64_t sp_batch_kernel_launches(const sp_batch* b);
+const char* sp_batch_last_error(const sp_batch* b);
+/* A group of bound, prepared batches stepped together from one graph (one branch each). */
+sp_group* sp_group_create(sp_batch** batches, int count, int* status);
+void sp_group_destroy(sp_group* g);
+int sp_group_step(sp_group* g, void* stream);
+const char* sp_group_last_error(const sp_group* g);
+
 /* Largest number of spectrum shells sp_spectrum_noalloc accepts: its accumulators are a fixed
  * file-scope device array of this many doubles (128 KiB).  2D grids up to n = 23168 fit, and
  * every 3D grid the engine indexes with 32 bits (n <= 1290). */

@@ -49,6 +49,23 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_last_error": (ctypes.c_char_p, [_vp]),
     "sp_create_error": (ctypes.c_char_p, []),
     "sp_spectrum_noalloc": (_i, [_vp, _i, _i, _i, _dp, _i, _vp]),
+    "sp_batch_create": (_vp, [_i, _i, _i, ctypes.POINTER(_i)]),
+    "sp_batch_destroy": (None, [_vp]),
+    "sp_batch_query_sizes": (_i, [_vp, ctypes.POINTER(ctypes.c_int64), _i]),
+    "sp_batch_bind": (_i, [_vp, _vp, _vp, _vp]),
+    "sp_batch_set_physics": (_i, [_vp, _dp, _d, _d, _d, _d]),
+    "sp_batch_set_step": (_i, [_vp, _dp, _dp, _vp]),
+    "sp_batch_prepare": (_i, [_vp, _vp]),
+    "sp_batch_step": (_i, [_vp, _vp]),
+    "sp_batch_sync_state": (_i, [_vp, _vp]),
+    "sp_batch_diagnostics": (_i, [_vp, _d, _d, _dp, _vp]),
+    "sp_batch_max_velocity": (_i, [_vp, _dp, _vp]),
+    "sp_batch_kernel_launches": (ctypes.c_int64, [_vp]),
+    "sp_batch_last_error": (ctypes.c_char_p, [_vp]),
+    "sp_group_create": (_vp, [ctypes.POINTER(_vp), _i, ctypes.POINTER(_i)]),
+    "sp_group_destroy": (None, [_vp]),
+    "sp_group_step": (_i, [_vp, _vp]),
+    "sp_group_last_error": (ctypes.c_char_p, [_vp]),
 }
 
 _LIB: ctypes.CDLL | None = None

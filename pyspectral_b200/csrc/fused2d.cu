@@ -39,42 +39,56 @@ cudaError_t attrs() {
 }
 
 template <typename T, int N>
-cudaError_t row(void* X, int kc, const void* tw, cudaStream_t st) {
+cudaError_t row(void* X, int kc, const void* tw, cudaStream_t st, int members, size_t xs) {
     using F = RowSingle<N>;
-    k_row_pass<T, N><<<N / F::B, F::THREADS, F::smem_bytes(sizeof(cplx<T>)), st>>>(
-        (Pair<T>*)X, kc, (const cplx<T>*)tw);
+    k_row_pass<T, N><<<dim3(N / F::B, members), F::THREADS, F::smem_bytes(sizeof(cplx<T>)), st>>>(
+        (Pair<T>*)X, kc, (const cplx<T>*)tw, xs);
     return cudaGetLastError();
 }
 
 template <typename T, int N>
 cudaError_t rmax(const void* X, int kc, const void* tw, unsigned long long* umax,
-                 cudaStream_t st) {
+                 cudaStream_t st, int members, size_t xs) {
     using F = RowPairs<N>;
-    k_row_max<T, N><<<(N / 2) / F::B, F::THREADS, F::smem_bytes(sizeof(Pair<T>)), st>>>(
-        (const Pair<T>*)X, kc, (const cplx<T>*)tw, umax);
+    k_row_max<T, N><<<dim3((N / 2) / F::B, members), F::THREADS,
+                      F::smem_bytes(sizeof(Pair<T>)), st>>>((const Pair<T>*)X, kc,
+                                                            (const cplx<T>*)tw, umax, xs);
     return cudaGetLastError();
 }
 
+struct ColArgs {
+    void* X;
+    int kc;
+    void* u0t;
+    void* acct;
+    const void* tab;
+    const void* P;
+    const void* tw;
+    cudaStream_t st;
+    int members;
+    size_t xs, us;
+    int ts;
+};
+
 template <typename T, int N, int STAGE>
-cudaError_t col_stage(void* X, int kc, void* u0t, void* acct, const void* tab, const void* P,
-                      const void* tw, cudaStream_t st) {
+cudaError_t col_stage(const ColArgs& a) {
     using F = Fused2D<N>;
-    const int grid = (kc + F::B - 1) / F::B;
-    k_col_pass<T, N, STAGE><<<grid, F::THREADS, F::template smem_bytes<Pair<T>>(), st>>>(
-        (Pair<T>*)X, kc, (cplx<T>*)u0t, (cplx<T>*)acct, (const T*)tab,
-        (const StepParams<T>*)P, (const cplx<T>*)tw);
+    const int grid = (a.kc + F::B - 1) / F::B;
+    k_col_pass<T, N, STAGE><<<dim3(grid, a.members), F::THREADS,
+                              F::template smem_bytes<Pair<T>>(), a.st>>>(
+        (Pair<T>*)a.X, a.kc, (cplx<T>*)a.u0t, (cplx<T>*)a.acct, (const T*)a.tab,
+        (const StepParams<T>*)a.P, (const cplx<T>*)a.tw, a.xs, a.us, a.ts);
     return cudaGetLastError();
 }
 
 template <typename T, int N>
-cudaError_t col(int stage, void* X, int kc, void* u0t, void* acct, const void* tab,
-                const void* P, const void* tw, cudaStream_t st) {
+cudaError_t col(int stage, const ColArgs& a) {
     switch (stage) {
-        case -1: return col_stage<T, N, -1>(X, kc, u0t, acct, tab, P, tw, st);
-        case 0: return col_stage<T, N, 0>(X, kc, u0t, acct, tab, P, tw, st);
-        case 1: return col_stage<T, N, 1>(X, kc, u0t, acct, tab, P, tw, st);
-        case 2: return col_stage<T, N, 2>(X, kc, u0t, acct, tab, P, tw, st);
-        case 3: return col_stage<T, N, 3>(X, kc, u0t, acct, tab, P, tw, st);
+        case -1: return col_stage<T, N, -1>(a);
+        case 0: return col_stage<T, N, 0>(a);
+        case 1: return col_stage<T, N, 1>(a);
+        case 2: return col_stage<T, N, 2>(a);
+        case 3: return col_stage<T, N, 3>(a);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -169,53 +183,79 @@ cudaError_t set_attributes(int n, int fp64) {
     return dispatch(n, fp64, [&]<typename T, int N>() { return attrs<T, N>(); });
 }
 
-cudaError_t row_pass(int n, int fp64, void* X, int kc, const void* tw, cudaStream_t st) {
-    return dispatch(n, fp64, [&]<typename T, int N>() { return row<T, N>(X, kc, tw, st); });
-}
-
-cudaError_t row_max(int n, int fp64, const void* X, int kc, const void* tw,
-                    unsigned long long* umax, cudaStream_t st) {
-    return dispatch(n, fp64,
-                    [&]<typename T, int N>() { return rmax<T, N>(X, kc, tw, umax, st); });
-}
-
-cudaError_t col_pass(int n, int fp64, int stage, void* X, int kc, void* u0t, void* acct,
-                     const void* tab, const void* params, const void* tw, cudaStream_t st) {
+cudaError_t row_pass(int n, int fp64, void* X, int kc, const void* tw, cudaStream_t st,
+                     int members, size_t x_stride) {
     return dispatch(n, fp64, [&]<typename T, int N>() {
-        return col<T, N>(stage, X, kc, u0t, acct, tab, params, tw, st);
+        return row<T, N>(X, kc, tw, st, members, x_stride);
     });
 }
 
-cudaError_t transpose_in(int fp64, const void* u0, void* u0t, int n, int kc, cudaStream_t st) {
-    dim3 grid((kc + 31) / 32, (n + 31) / 32), block(32, 8);
+cudaError_t row_max(int n, int fp64, const void* X, int kc, const void* tw,
+                    unsigned long long* umax, cudaStream_t st, int members, size_t x_stride) {
+    return dispatch(n, fp64, [&]<typename T, int N>() {
+        return rmax<T, N>(X, kc, tw, umax, st, members, x_stride);
+    });
+}
+
+cudaError_t col_pass(int n, int fp64, int stage, void* X, int kc, void* u0t, void* acct,
+                     const void* tab, const void* params, const void* tw, cudaStream_t st,
+                     int members, size_t x_stride, size_t u_stride, int tab_stride) {
+    ColArgs a{X, kc, u0t, acct, tab, params, tw, st, members, x_stride, u_stride, tab_stride};
+    return dispatch(n, fp64, [&]<typename T, int N>() { return col<T, N>(stage, a); });
+}
+
+cudaError_t transpose_in(int fp64, const void* u0, void* u0t, int n, int kc, cudaStream_t st,
+                         int members, size_t u0_stride, size_t u_stride) {
+    dim3 grid((kc + 31) / 32, (n + 31) / 32, members), block(32, 8);
     const int nh = n / 2 + 1;
     if (fp64)
         k_transpose_in<double><<<grid, block, 0, st>>>((const cplx<double>*)u0,
-                                                       (cplx<double>*)u0t, n, nh, kc);
+                                                       (cplx<double>*)u0t, n, nh, kc, u0_stride,
+                                                       u_stride);
     else
         k_transpose_in<float><<<grid, block, 0, st>>>((const cplx<float>*)u0, (cplx<float>*)u0t,
-                                                      n, nh, kc);
+                                                      n, nh, kc, u0_stride, u_stride);
     return cudaGetLastError();
 }
 
-cudaError_t transpose_out(int fp64, const void* u0t, void* u0, int n, int kc, cudaStream_t st) {
-    dim3 grid((kc + 31) / 32, (n + 31) / 32), block(32, 8);
+cudaError_t transpose_out(int fp64, const void* u0t, void* u0, int n, int kc, cudaStream_t st,
+                          int members, size_t u_stride, size_t u0_stride) {
+    dim3 grid((kc + 31) / 32, (n + 31) / 32, members), block(32, 8);
     const int nh = n / 2 + 1;
     if (fp64)
         k_transpose_out<double><<<grid, block, 0, st>>>((const cplx<double>*)u0t,
-                                                        (cplx<double>*)u0, n, nh, kc);
+                                                        (cplx<double>*)u0, n, nh, kc, u_stride,
+                                                        u0_stride);
     else
         k_transpose_out<float><<<grid, block, 0, st>>>((const cplx<float>*)u0t,
-                                                       (cplx<float>*)u0, n, nh, kc);
+                                                       (cplx<float>*)u0, n, nh, kc, u_stride,
+                                                       u0_stride);
     return cudaGetLastError();
 }
 
-cudaError_t mask2d(int fp64, void* u0, int n, cudaStream_t st) {
+cudaError_t mask2d(int fp64, void* u0, int n, cudaStream_t st, int members) {
     const int nh = n / 2 + 1;
     const uint32_t fsc = (uint32_t)n * (uint32_t)nh;
-    const unsigned grid = (fsc + 255) / 256;
+    const dim3 grid((fsc + 255) / 256, members);
     if (fp64) k_mask2d<double><<<grid, 256, 0, st>>>((cplx<double>*)u0, n, nh, fsc);
     else k_mask2d<float><<<grid, 256, 0, st>>>((cplx<float>*)u0, n, nh, fsc);
+    return cudaGetLastError();
+}
+
+cudaError_t reduce_t(int fp64, const void* u0t, int n, int kc, size_t u_stride, int members,
+                     double klo, double khi, double* partials, int nblk, double* out,
+                     cudaStream_t st) {
+    const double inv_norm = 1.0 / std::pow((double)n, 4.0);
+    const dim3 grid(nblk, members);
+    if (fp64)
+        k_reduce_t<double><<<grid, 256, 0, st>>>((const cplx<double>*)u0t, n, kc, u_stride,
+                                                 inv_norm, klo * klo, khi * khi, partials);
+    else
+        k_reduce_t<float><<<grid, 256, 0, st>>>((const cplx<float>*)u0t, n, kc, u_stride,
+                                                inv_norm, klo * klo, khi * khi, partials);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_reduce_t_finish<<<members, 256, 0, st>>>(partials, nblk, out);
     return cudaGetLastError();
 }
 

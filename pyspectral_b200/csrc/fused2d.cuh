@@ -23,6 +23,7 @@
 
 #include "common.cuh"
 #include "fft_block.cuh"
+#include "reduce.cuh"
 
 namespace sp {
 
@@ -84,10 +85,13 @@ struct RowSingle {
     static constexpr size_t smem_bytes(size_t elem) { return (size_t)B * FftPlan<N>::SMEM * elem; }
 };
 
+// Batched launches: blockIdx.y selects the member; each member's arrays start `stride`
+// elements after the previous member's (stride 0 for a single run).
 template <typename T, int N>
 __global__ void __launch_bounds__(RowSingle<N>::THREADS, 2) k_row_pass(Pair<T>* __restrict__ X,
                                                                       int kc,
-                                                                      const cplx<T>* __restrict__ tw) {
+                                                                      const cplx<T>* __restrict__ tw,
+                                                                      size_t x_stride) {
     using F = RowSingle<N>;
     constexpr int TT = F::T;
     constexpr int RI = first_radix<N, true>();   // inverse input pattern
@@ -98,6 +102,7 @@ __global__ void __launch_bounds__(RowSingle<N>::THREADS, 2) k_row_pass(Pair<T>* 
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
     const int row = blockIdx.x * F::B + sub;  // n is a multiple of B
     const int p = row >> 1, half = row & 1;
+    X += blockIdx.y * x_stride;
 
     cplx<T> v[16];
 #pragma unroll
@@ -135,7 +140,8 @@ template <typename T, int N>
 __global__ void __launch_bounds__(RowPairs<N>::THREADS) k_row_max(const Pair<T>* __restrict__ X,
                                                                  int kc,
                                                                  const cplx<T>* __restrict__ tw,
-                                                                 unsigned long long* umax) {
+                                                                 unsigned long long* umax,
+                                                                 size_t x_stride) {
     using F = RowPairs<N>;
     constexpr int TT = F::T;
     constexpr int RI = first_radix<N, true>();
@@ -143,6 +149,8 @@ __global__ void __launch_bounds__(RowPairs<N>::THREADS) k_row_max(const Pair<T>*
     const int sub = threadIdx.x / TT, t = threadIdx.x % TT;
     Pair<T>* sm = reinterpret_cast<Pair<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
     const int p = blockIdx.x * F::B + sub;
+    X += blockIdx.y * x_stride;
+    umax += 2 * blockIdx.y;
     Pair<T> v[16];
 #pragma unroll
     for (int g = 0; g < 16 / RI; ++g)
@@ -202,7 +210,7 @@ template <typename T, int N, int STAGE>
 __global__ void __launch_bounds__(Fused2D<N>::THREADS) k_col_pass(
     Pair<T>* __restrict__ X, int kc, cplx<T>* __restrict__ u0t, cplx<T>* __restrict__ acct,
     const T* __restrict__ tab, const StepParams<T>* __restrict__ P,
-    const cplx<T>* __restrict__ tw) {
+    const cplx<T>* __restrict__ tw, size_t x_stride, size_t u_stride, int tab_stride) {
     using F = Fused2D<N>;
     constexpr int TT = F::T;
     constexpr int RF0 = first_radix<N, false>();  // forward input pattern
@@ -214,7 +222,11 @@ __global__ void __launch_bounds__(Fused2D<N>::THREADS) k_col_pass(
     Pair<T>* sm = reinterpret_cast<Pair<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
     const int ky = blockIdx.x * F::B + sub;
     const bool active = ky < kc;  // inactive sub-blocks still take part in every barrier
-    const StepParams<T> p = *P;
+    X += blockIdx.y * x_stride;
+    u0t += blockIdx.y * u_stride;
+    acct += blockIdx.y * u_stride;
+    tab += blockIdx.y * tab_stride;
+    const StepParams<T> p = P[blockIdx.y];
     const T kyr = (T)ky;
     const int nh = N / 2 + 1;
 
@@ -275,8 +287,10 @@ __global__ void __launch_bounds__(Fused2D<N>::THREADS) k_col_pass(
 template <typename T>
 __global__ void __launch_bounds__(256) k_transpose_in(const cplx<T>* __restrict__ u0,
                                                       cplx<T>* __restrict__ u0t, int n, int nh,
-                                                      int kc) {
+                                                      int kc, size_t u0_stride, size_t u_stride) {
     __shared__ cplx<T> tile[32][33];
+    u0 += blockIdx.z * u0_stride;
+    u0t += blockIdx.z * u_stride;
     const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;  // i = row (x index), j = ky
     for (int r = threadIdx.y; r < 32; r += 8) {
         int i = i0 + r, j = j0 + threadIdx.x;
@@ -292,8 +306,10 @@ __global__ void __launch_bounds__(256) k_transpose_in(const cplx<T>* __restrict_
 template <typename T>
 __global__ void __launch_bounds__(256) k_transpose_out(const cplx<T>* __restrict__ u0t,
                                                        cplx<T>* __restrict__ u0, int n, int nh,
-                                                       int kc) {
+                                                       int kc, size_t u_stride, size_t u0_stride) {
     __shared__ cplx<T> tile[32][33];
+    u0t += blockIdx.z * u_stride;
+    u0 += blockIdx.z * u0_stride;
     const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
     for (int r = threadIdx.y; r < 32; r += 8) {
         int j = j0 + r, i = i0 + threadIdx.x;
@@ -312,10 +328,61 @@ __global__ void __launch_bounds__(256) k_mask2d(cplx<T>* __restrict__ u0, int n,
                                                 uint32_t fsc) {
     uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= fsc) return;
+    u0 += (size_t)blockIdx.y * fsc;
     uint32_t i = idx / (uint32_t)nh, j = idx - i * (uint32_t)nh;
     int kxi = signed_k((int)i, n);
     int akx = kxi < 0 ? -kxi : kxi;
     if (!(3 * akx < n && 3 * (int)j < n)) u0[idx] = mk<T>(0, 0);
+}
+
+// Spectral sums of each member's transposed state (kept modes only; the others are zero):
+// partials[(m * nblk + b) * 4 + q], q = energy, enstrophy, palinstrophy, band energy (x2, the
+// 1/2 is applied when the partials are summed).  2D: energy density |w|^2 / k^2.
+template <typename T>
+__global__ void __launch_bounds__(256) k_reduce_t(const cplx<T>* __restrict__ u0t, int n, int kc,
+                                                  size_t u_stride, double inv_norm, double klo2,
+                                                  double khi2, double* __restrict__ partials) {
+    __shared__ double smem[4 * 32];
+    const cplx<T>* st = u0t + blockIdx.y * u_stride;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    const uint32_t total = (uint32_t)kc * (uint32_t)n;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += gridDim.x * blockDim.x) {
+        const uint32_t ky = e / (uint32_t)n, i = e - ky * (uint32_t)n;
+        const int kxi = signed_k((int)i, n);
+        const int akx = kxi < 0 ? -kxi : kxi;
+        if (3 * akx >= n) continue;
+        const cplx<T> z = st[e];
+        const double kx = (double)kxi, kyd = (double)ky, k2 = kx * kx + kyd * kyd;
+        const double w = (ky == 0 || 2 * (int)ky == n) ? inv_norm : 2.0 * inv_norm;
+        const double d = ((double)z.x * z.x + (double)z.y * z.y) * w;
+        const double de = k2 > 0.0 ? d * (1.0 / k2) : 0.0;
+        v[0] += de;
+        v[1] += d;
+        v[2] += d * k2;
+        if (k2 >= klo2 && k2 <= khi2) v[3] += de;
+    }
+    block_sum<4>(v, smem);
+    if (threadIdx.x == 0) {
+        double* out = partials + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 4;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) out[q] = v[q];
+    }
+}
+
+// out[m * 4 + q] = 0.5 * sum over member m's nblk partial rows, fixed order.
+__global__ void __launch_bounds__(256) k_reduce_t_finish(const double* __restrict__ partials,
+                                                         int nblk, double* __restrict__ out) {
+    __shared__ double smem[4 * 32];
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    const double* pm = partials + (size_t)blockIdx.x * nblk * 4;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[q] += pm[b * 4 + q];
+    block_sum<4>(v, smem);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) out[blockIdx.x * 4 + q] = 0.5 * v[q];
 }
 
 }  // namespace sp

@@ -19,15 +19,29 @@ cudaError_t set_attributes(int n, int fp64);
 int twiddle_table_size(int n);
 void fill_twiddles(int n, double* out);
 
-cudaError_t row_pass(int n, int fp64, void* X, int kc, const void* tw, cudaStream_t st);
+// Batched forms: `members` independent runs of the same grid, member m's arrays `*_stride`
+// elements after member m-1's (X in Pair units, u0/u0t/acct in complex units, tab in reals).
+cudaError_t row_pass(int n, int fp64, void* X, int kc, const void* tw, cudaStream_t st,
+                     int members = 1, size_t x_stride = 0);
 cudaError_t row_max(int n, int fp64, const void* X, int kc, const void* tw,
-                    unsigned long long* umax, cudaStream_t st);
-// stage -1: build the stage-0 inputs from u0t; 0..3: Lawson stage
+                    unsigned long long* umax, cudaStream_t st, int members = 1,
+                    size_t x_stride = 0);
+// stage -1: build the stage-0 inputs from u0t; 0..3: Lawson stage.  params/tab: one
+// StepParams and one table (tab_stride reals) per member.
 cudaError_t col_pass(int n, int fp64, int stage, void* X, int kc, void* u0t, void* acct,
-                     const void* tab, const void* params, const void* tw, cudaStream_t st);
-cudaError_t transpose_in(int fp64, const void* u0, void* u0t, int n, int kc, cudaStream_t st);
-cudaError_t transpose_out(int fp64, const void* u0t, void* u0, int n, int kc, cudaStream_t st);
-cudaError_t mask2d(int fp64, void* u0, int n, cudaStream_t st);
+                     const void* tab, const void* params, const void* tw, cudaStream_t st,
+                     int members = 1, size_t x_stride = 0, size_t u_stride = 0,
+                     int tab_stride = 0);
+cudaError_t transpose_in(int fp64, const void* u0, void* u0t, int n, int kc, cudaStream_t st,
+                         int members = 1, size_t u0_stride = 0, size_t u_stride = 0);
+cudaError_t transpose_out(int fp64, const void* u0t, void* u0, int n, int kc, cudaStream_t st,
+                          int members = 1, size_t u_stride = 0, size_t u0_stride = 0);
+cudaError_t mask2d(int fp64, void* u0, int n, cudaStream_t st, int members = 1);
+// Energy, enstrophy, palinstrophy, band energy of every member's transposed state into
+// out[m * 4 + q]; partials: members * nblk * 4 doubles of scratch.
+cudaError_t reduce_t(int fp64, const void* u0t, int n, int kc, size_t u_stride, int members,
+                     double klo, double khi, double* partials, int nblk, double* out,
+                     cudaStream_t st);
 
 }  // namespace fused
 }  // namespace sp

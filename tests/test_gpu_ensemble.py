@@ -1,0 +1,139 @@
+"""Batched ensembles of uneven grid sizes against single runs and the oracle (GPU)."""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle.numpy_oracle import OracleSolver
+from pyspectral_b200 import BackendUnavailable, Config, initial
+from pyspectral_b200.registry import get
+
+pytestmark = pytest.mark.gpu
+FUSED = "b200/fused-fft-graph"
+
+
+def _members(dtype: str) -> list[Config]:
+    out = []
+    for n in (32, 64, 128):
+        for j in range(2):
+            out.append(Config(n=n, dim=2, nu=2e-3 * (1 + j), alpha=0.1, alpha_kmax=2.0,
+                              force_amp=0.2 + 0.1 * j, force_klo=3, force_khi=5, dtype=dtype))
+    return out
+
+
+def _ics(members: list[Config]) -> list[np.ndarray]:
+    return [initial.random_phase_2d(c.n, k0=c.n / 10, seed=7 + i) for i, c in enumerate(members)]
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_members_equal_single_runs_bit_for_bit(dtype):
+    from pyspectral_b200.ensemble import Ensemble
+
+    cfgs = _members(dtype)
+    ics = _ics(cfgs)
+    ens = Ensemble(cfgs)
+    ens.set_states(ics)
+    dts = [np.array([1e-3 * (1 + 0.1 * i + 0.05 * k) for i in range(len(cfgs))]) for k in range(6)]
+    amps = [np.array([0.2 + 0.02 * i + 0.01 * k for i in range(len(cfgs))]) for k in range(6)]
+    for k in range(6):
+        ens.set_forcing_amplitudes(amps[k])
+        ens.step(dts[k])
+    for i, c in enumerate(cfgs):
+        s = get(FUSED).make(c)
+        s.set_state(ics[i])
+        for k in range(6):
+            s.set_forcing_amplitude(amps[k][i])
+            s.step(dts[k][i])
+        assert np.array_equal(ens.get_state(i), s.get_state()), i
+        assert ens.t[i] == pytest.approx(s.t)
+
+
+def test_batched_diagnostics_and_cfl_match_single_runs():
+    from pyspectral_b200.ensemble import Ensemble
+
+    cfgs = _members("float64")
+    ics = _ics(cfgs)
+    ens = Ensemble(cfgs)
+    ens.set_states(ics)
+    ens.step(1e-3)
+    d = ens.diagnostics(3, 5)
+    u = ens.max_velocity_sum()
+    for i, c in enumerate(cfgs):
+        s = get(FUSED).make(c)
+        s.set_state(ics[i])
+        s.step(1e-3)
+        ref = s.diag.all(s.state_native(), 3, 5)
+        np.testing.assert_allclose(d[i], [ref["energy"], ref["enstrophy"], ref["palinstrophy"],
+                                          ref["band_energy"]], rtol=1e-12)
+        assert u[i] == pytest.approx(s.diag.max_velocity_sum(s.state_native()), rel=1e-12)
+
+
+def test_small_member_matches_oracle():
+    from pyspectral_b200.ensemble import Ensemble
+
+    c = Config(n=32, dim=2, nu=0.01, alpha=0.5, alpha_kmax=2.0, force_amp=0.3, force_klo=1,
+               force_khi=2.5, dtype="float64")
+    big = Config(n=256, dim=2, nu=1e-3, dtype="float64")
+    ic = initial.to_spectral(initial.random_2d(32, k0=4), 2)
+    ens = Ensemble([c, big])
+    ens.set_states([ic, initial.random_phase_2d(256, k0=8, seed=1)])
+    ref = OracleSolver(32, 2, nu=0.01, alpha=0.5, alpha_kmax=2.0, force_amp=0.3, force_klo=1,
+                       force_khi=2.5)
+    ref.set_state(ic)
+    for k in range(5):
+        ens.step([0.01, 1e-3])
+        ref.step(0.01)
+    ens.set_forcing_amplitudes([0.1, 0.0])
+    ref.set_forcing_amplitude(0.1)
+    for k in range(3):
+        ens.step([0.007, 1e-3])
+        ref.step(0.007)
+    r = ref.get_state()
+    assert np.abs(ens.get_state(0) - r).max() / np.abs(r).max() < 1e-12
+
+
+def test_constant_power_cfl_run_matches_single_run_driver():
+    from pyspectral_b200.ensemble import Ensemble
+    from pyspectral_b200.simulate import run_steps
+
+    cfgs = [Config(n=n, dim=2, nu=1e-3, alpha=0.1, alpha_kmax=2, force_klo=3, force_khi=5,
+                   dtype="float64") for n in (64, 128, 128)]
+    ics = _ics(cfgs)
+    ens = Ensemble(cfgs)
+    ens.set_states(ics)
+    hist = ens.run_steps(25, cfl=0.5, target_power=1e-3)
+    assert hist.shape == (25, 3) and np.all(hist > 0)
+    for i, c in enumerate(cfgs):
+        s = get(FUSED).make(c)
+        s.set_state(ics[i])
+        dts = run_steps(s, 25, cfl=0.5, target_power=1e-3)
+        np.testing.assert_allclose(hist[:, i], dts, rtol=1e-12)
+        r = s.get_state()
+        assert np.abs(ens.get_state(i) - r).max() / np.abs(r).max() < 1e-12
+
+
+def test_one_graph_step_launches_eight_kernels_per_class():
+    from pyspectral_b200.ensemble import Ensemble
+
+    ens = Ensemble(_members("float32"))
+    ens.set_states(_ics(ens.members))
+    ens.step(1e-3)
+    before = ens.kernel_launches
+    ens.step(1e-3)
+    assert ens.kernel_launches - before == 8 * len(ens.classes) == 24
+
+
+def test_ensemble_rejects_unsupported_members():
+    from pyspectral_b200.ensemble import Ensemble
+
+    with pytest.raises(BackendUnavailable):
+        Ensemble([Config(n=48, dim=2)])
+    with pytest.raises(BackendUnavailable):
+        Ensemble([Config(n=32, dim=3)])
+    with pytest.raises(ValueError):
+        Ensemble([Config(n=32, dim=2, alpha=0.1), Config(n=32, dim=2, alpha=0.2)])
+    assert math.isclose(__import__("pyspectral_b200.ensemble", fromlist=["x"]).nu_for_kmax_eta(
+        384, 1e-3, 11.0), (121e-3) ** (1 / 3) * (1 / 128) ** 2)
