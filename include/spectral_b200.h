@@ -211,6 +211,14 @@ void sp_group_destroy(sp_group* g);
 int sp_group_step(sp_group* g, void* stream);
 const char* sp_group_last_error(const sp_group* g);
 
+/* ---------------------------------------------------------------- tensor-core tiles
+ * Check of the BF16 tcgen05 tile path the closure network uses (no reference counterpart):
+ * D[128 x N] (fp32, row-major) = A * B^T with A = [128 x K] (a_mn = 0) or given transposed as
+ * [K x 128] (a_mn = 1), B = [N x K] (b_mn = 0) or [K x N] (b_mn = 1), bf16 row-major device
+ * arrays; N and K multiples of 16 in 16..256.  Synchronises `stream`. */
+int sp_mma_tile_check(const void* A, const void* B, float* D, int N, int K, int a_mn, int b_mn,
+                      void* stream);
+
 /* Largest number of spectrum shells sp_spectrum_noalloc accepts: its accumulators are a fixed
  * file-scope device array of this many doubles (128 KiB).  2D grids up to n = 23168 fit, and
  * every 3D grid the engine indexes with 32 bits (n <= 1290). */

@@ -66,6 +66,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_group_destroy": (None, [_vp]),
     "sp_group_step": (_i, [_vp, _vp]),
     "sp_group_last_error": (ctypes.c_char_p, [_vp]),
+    "sp_mma_tile_check": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _vp]),
 }
 
 _LIB: ctypes.CDLL | None = None
