@@ -219,6 +219,80 @@ const char* sp_group_last_error(const sp_group* g);
 int sp_mma_tile_check(const void* A, const void* B, float* D, int N, int K, int a_mn, int b_mn,
                       void* stream);
 
+/* ---------------------------------------------------------------- spectral helpers
+ * Dealiased 2D nonlinear term N(state) (Basdevant form, no linear terms) of a spectral state in
+ * u0 layout, written to `out` (same layout).  Replaces NumpySolver.nonlinear
+ * (src/pyspectral/backends/numpy_ref.py:75-96, 2D branch).  Needs a bound 2D solver created
+ * with SP_FFT_CUFFT; uses the work array as scratch and rebuilds the next stage's inputs from u0
+ * afterwards, so stepping may continue. */
+int sp_nonlinear(sp_solver* s, const void* state, void* out, void* stream);
+
+/* pad_spectrum (src/pyspectral/validation.py:24-35) on the device: zero-pad or truncate an r2c
+ * spectrum of grid n_src to grid n_dst (keeping |k| < min(n_src, n_dst)/2, rescaled by
+ * (n_dst/n_src)^dim); dealias != 0 also applies n_dst's 2/3 mask, the sharp spectral filter of
+ * the learned closure.  dim 2 or 3, fp32 or fp64 complex, src and dst must not overlap. */
+int sp_filter_spectrum(const void* src, int n_src, void* dst, int n_dst, int dim, int fp64,
+                       int dealias, void* stream);
+
+/* ---------------------------------------------------------------- learned closure
+ * No reference counterpart.  A per-point network 75 -> 64 -> 64 -> 64 -> 1 (GELU, tanh form)
+ * maps the 5 x 5 stencils of the filtered vorticity and of its x and y derivatives to the
+ * subgrid term S = F[N(omega)] - N_c(F[omega]) of a coarse 2D run (F = sp_filter_spectrum with
+ * dealiasing, N and N_c the fine and coarse nonlinear terms).  Layers 1-3 are BF16 tcgen05
+ * GEMMs with FP32 accumulation; the output layer is FP32.  Parameters (fp32, 15440 values):
+ * W1, W2, W3 as [64][80] row-major with the bias in column 75 (W1) or 64 (W2, W3) and zero
+ * padding, then w4[80] with the bias at index 64.  Axis x is the first (row) axis of a field,
+ * y the contiguous one; feature f * 25 + (dx + 2) * 5 + (dy + 2) is field f at offset (dx, dy). */
+typedef struct sp_closure sp_closure;
+
+int sp_closure_param_count(void);
+/* n: coarse grid, a power of two in 128..4096; capacity: snapshot-bank entries of 4 n^2 floats
+ * (omega, omega_x, omega_y, S in physical space). */
+sp_closure* sp_closure_create(int n, int capacity, int* status);
+void sp_closure_destroy(sp_closure* c);
+const char* sp_closure_last_error(const sp_closure* c);
+int64_t sp_closure_kernel_launches(const sp_closure* c);
+/* Host fp32 parameters; resets the Adam moments, the step counter and the loss record. */
+int sp_closure_set_params(sp_closure* c, const float* host);
+int sp_closure_get_params(sp_closure* c, float* host);
+/* Gradient of the last sp_closure_grad / training step (15440 floats). */
+int sp_closure_get_grad(sp_closure* c, float* host);
+/* Network inputs are field * inscale[f]; its output times outscale is S.  clip != 0 zeroes
+ * predictions with S * omega > 0 (local enstrophy backscatter) at inference. */
+int sp_closure_set_scales(sp_closure* c, const float* inscale3, float outscale, int clip);
+int sp_closure_get_scales(const sp_closure* c, float* out5);
+/* Adam with linear warm-up over `warmup` steps and cosine decay to lr_min at total_steps. */
+int sp_closure_set_adam(sp_closure* c, double lr, double lr_min, double beta1, double beta2,
+                        double eps, int total_steps, int warmup);
+/* Snapshot bank: load `count` host entries, append one from device spectra (coarse u0 layout,
+ * fp32: the filtered vorticity, the filtered fine nonlinear term, the coarse nonlinear term of
+ * the filtered vorticity), read one entry back, count, clear. */
+int sp_closure_bank_load(sp_closure* c, const float* host, int count);
+int sp_closure_add_snapshot(sp_closure* c, const void* wbar_hat, const void* fine_nl_hat,
+                            const void* coarse_nl_hat, void* stream);
+int sp_closure_bank_read(sp_closure* c, int index, float* host);
+int sp_closure_bank_count(const sp_closure* c);
+int sp_closure_bank_reset(sp_closure* c);
+/* Mean-squared-error gradient over batch_tiles tiles of 128 points (a row segment of one bank
+ * entry each, drawn by a counter hash of (seed, step, tile)), without an update. */
+int sp_closure_grad(sp_closure* c, int64_t step, int batch_tiles, uint64_t seed, void* stream);
+/* `steps` Adam steps at batch_tiles tiles each (graph-replayed in chunks); synchronises. */
+int sp_closure_train(sp_closure* c, int steps, int batch_tiles, uint64_t seed, void* stream);
+int64_t sp_closure_step_count(const sp_closure* c);
+/* Mean loss of steps first .. first+count-1 (the last 65536 steps are kept). */
+int sp_closure_losses(sp_closure* c, int64_t first, int count, float* host);
+/* S at every point of an n x n field: inputs omega, omega_x, omega_y at fields + f*field_stride
+ * (row stride row_stride floats), output rows of out_row_stride floats; synchronises. */
+int sp_closure_infer(sp_closure* c, const float* fields, int64_t field_stride, int row_stride,
+                     float* out, int out_row_stride, void* stream);
+/* Attach a closure to a 2D fp32 SP_FFT_CUFFT solver of the same grid before sp_bind: every
+ * stage then adds the network's S to the nonlinear term (the sizes sp_query_sizes reports grow
+ * to six work fields).  The closure must outlive the solver. */
+int sp_attach_closure(sp_solver* s, sp_closure* c);
+/* Reports (and clears) a tensor-core wait that timed out in a closure kernel launched by a
+ * solver step; synchronises `stream`. */
+int sp_closure_check(sp_closure* c, void* stream);
+
 /* Largest number of spectrum shells sp_spectrum_noalloc accepts: its accumulators are a fixed
  * file-scope device array of this many doubles (128 KiB).  2D grids up to n = 23168 fit, and
  * every 3D grid the engine indexes with 32 bits (n <= 1290). */

@@ -26,6 +26,7 @@ SZ_MODES, SZ_NCOMP, SZ_NWORK, SZ_NINV, SZ_NFWD = 0, 1, 2, 3, 4
 SZ_STATE_BYTES, SZ_WORK_BYTES, SZ_AUX_BYTES, SZ_FFTWS_BYTES, SZ_NSHELL, SZ_COUNT = 5, 6, 7, 8, 9, 10
 
 _vp, _i, _d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+_i64, _u64, _f = ctypes.c_int64, ctypes.c_uint64, ctypes.c_float
 _dp = ctypes.POINTER(ctypes.c_double)
 
 # name -> (restype, argtypes); the exported C ABI
@@ -67,6 +68,31 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_group_step": (_i, [_vp, _vp]),
     "sp_group_last_error": (ctypes.c_char_p, [_vp]),
     "sp_mma_tile_check": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _vp]),
+    "sp_nonlinear": (_i, [_vp, _vp, _vp, _vp]),
+    "sp_filter_spectrum": (_i, [_vp, _i, _vp, _i, _i, _i, _i, _vp]),
+    "sp_closure_param_count": (_i, []),
+    "sp_closure_create": (_vp, [_i, _i, ctypes.POINTER(_i)]),
+    "sp_closure_destroy": (None, [_vp]),
+    "sp_closure_last_error": (ctypes.c_char_p, [_vp]),
+    "sp_closure_kernel_launches": (_i64, [_vp]),
+    "sp_closure_set_params": (_i, [_vp, _vp]),
+    "sp_closure_get_params": (_i, [_vp, _vp]),
+    "sp_closure_get_grad": (_i, [_vp, _vp]),
+    "sp_closure_set_scales": (_i, [_vp, _vp, _f, _i]),
+    "sp_closure_get_scales": (_i, [_vp, _vp]),
+    "sp_closure_set_adam": (_i, [_vp, _d, _d, _d, _d, _d, _i, _i]),
+    "sp_closure_bank_load": (_i, [_vp, _vp, _i]),
+    "sp_closure_add_snapshot": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "sp_closure_bank_read": (_i, [_vp, _i, _vp]),
+    "sp_closure_bank_count": (_i, [_vp]),
+    "sp_closure_bank_reset": (_i, [_vp]),
+    "sp_closure_grad": (_i, [_vp, _i64, _i, _u64, _vp]),
+    "sp_closure_train": (_i, [_vp, _i, _i, _u64, _vp]),
+    "sp_closure_step_count": (_i64, [_vp]),
+    "sp_closure_losses": (_i, [_vp, _i64, _i, _vp]),
+    "sp_closure_infer": (_i, [_vp, _vp, _i64, _i, _vp, _i, _vp]),
+    "sp_attach_closure": (_i, [_vp, _vp]),
+    "sp_closure_check": (_i, [_vp, _vp]),
 }
 
 _LIB: ctypes.CDLL | None = None

@@ -48,9 +48,21 @@ __device__ __forceinline__ void velocity2(const Mode2<T>& m, cplx<T> w, T scale,
     v = scl(m.kx, mul_mi(psi));
 }
 
+// Closure layout of the 2D work array (a coarse run with the learned closure attached): slots
+// [S, u, v, omega, d omega/dx, d omega/dy]; the plain layout is [u, v].  The vorticity and its
+// gradient are the closure network's inputs, S its output.
+template <typename T>
+__device__ __forceinline__ void omega_set(const Mode2<T>& m, cplx<T> w, T scale, cplx<T>& o,
+                                          cplx<T>& ox, cplx<T>& oy) {
+    const T s = m.keep ? scale : (T)0;
+    o = scl(s, w);
+    ox = scl(m.kx * s, mul_i(w));
+    oy = scl(m.ky * s, mul_i(w));
+}
+
 // Loads a state: dealiases u0 in place (the host-side check_state mask of base.py:134-139, done
 // on the device) and writes the stage-0 inverse-FFT inputs.
-template <typename T>
+template <typename T, bool CL = false>
 __global__ void __launch_bounds__(kBlock) k_pre2d(cplx<T>* __restrict__ u0,
                                                   cplx<T>* __restrict__ W, int n, int nh,
                                                   uint32_t fsc,
@@ -60,18 +72,71 @@ __global__ void __launch_bounds__(kBlock) k_pre2d(cplx<T>* __restrict__ u0,
     const T scale = P->scale;
     uint32_t i = idx0 / (uint32_t)nh;
     uint32_t j = idx0 - i * (uint32_t)nh;
-    cplx<T> w[2], u[2], v[2];
+    cplx<T> w[2], u[2], v[2], o[2], ox[2], oy[2];
     ld2(u0 + idx0, w[0], w[1]);
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
         Mode2<T> m = mode2<T>((int)i, (int)j, n);
         if (!m.keep) w[e] = mk<T>(0, 0);
         velocity2(m, w[e], scale, u[e], v[e]);
+        if (CL) omega_set(m, w[e], scale, o[e], ox[e], oy[e]);
         if (++j == (uint32_t)nh) { j = 0; ++i; }
     }
     st2(u0 + idx0, w[0], w[1]);
+    cplx<T>* Wuv = CL ? W + fsc : W;
+    st2(Wuv + idx0, u[0], u[1]);
+    st2(Wuv + fsc + idx0, v[0], v[1]);
+    if (CL) {
+        st2(W + 3 * (size_t)fsc + idx0, o[0], o[1]);
+        st2(W + 4 * (size_t)fsc + idx0, ox[0], ox[1]);
+        st2(W + 5 * (size_t)fsc + idx0, oy[0], oy[1]);
+    }
+}
+
+// Nonlinear term of a given state (no update): the velocity pair of `state` (left untouched)
+// into the plain work layout ...
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_nl_pre2d(const cplx<T>* __restrict__ state,
+                                                     cplx<T>* __restrict__ W, int n, int nh,
+                                                     uint32_t fsc,
+                                                     const StepParams<T>* __restrict__ P) {
+    uint32_t idx0 = 2u * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (idx0 >= fsc) return;
+    const T scale = P->scale;
+    uint32_t i = idx0 / (uint32_t)nh;
+    uint32_t j = idx0 - i * (uint32_t)nh;
+    cplx<T> w[2], u[2], v[2];
+    ld2(state + idx0, w[0], w[1]);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        Mode2<T> m = mode2<T>((int)i, (int)j, n);
+        velocity2(m, w[e], scale, u[e], v[e]);
+        if (++j == (uint32_t)nh) { j = 0; ++i; }
+    }
     st2(W + idx0, u[0], u[1]);
     st2(W + fsc + idx0, v[0], v[1]);
+}
+
+// ... and, after the transforms and the products, the dealiased Basdevant term into `out`.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_nl_post2d(const cplx<T>* __restrict__ W,
+                                                      cplx<T>* __restrict__ out, int n, int nh,
+                                                      uint32_t fsc) {
+    uint32_t idx0 = 2u * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (idx0 >= fsc) return;
+    cplx<T> A[2], B[2], N[2];
+    ld2(W + idx0, A[0], A[1]);
+    ld2(W + fsc + idx0, B[0], B[1]);
+    uint32_t i = idx0 / (uint32_t)nh;
+    uint32_t j = idx0 - i * (uint32_t)nh;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        Mode2<T> m = mode2<T>((int)i, (int)j, n);
+        N[e] = mk<T>(0, 0);
+        if (m.keep) N[e] = axpy(m.kx * m.ky, A[e], scl(m.kx * m.kx - m.ky * m.ky, B[e]));
+        if (++j == (uint32_t)nh) { j = 0; ++i; }
+    }
+    st2(out + idx0, N[0], N[1]);
 }
 
 // physical space, in place over the padded real fields: (u, v) -> (v^2 - u^2, u v)
@@ -89,7 +154,7 @@ __global__ void __launch_bounds__(kBlock) k_phys2d(T* __restrict__ R, uint32_t f
     st4(R + fsr + p, b);
 }
 
-template <typename T, int STAGE>
+template <typename T, int STAGE, bool CL = false>
 __global__ void __launch_bounds__(kBlock) k_post2d(cplx<T>* __restrict__ W,
                                                    cplx<T>* __restrict__ u0,
                                                    cplx<T>* __restrict__ acc,
@@ -99,9 +164,11 @@ __global__ void __launch_bounds__(kBlock) k_post2d(cplx<T>* __restrict__ W,
     uint32_t idx0 = 2u * (blockIdx.x * blockDim.x + threadIdx.x);
     if (idx0 >= fsc) return;
     const StepParams<T> p = *P;
-    cplx<T> A[2], B[2], U[2], C[2], nu_[2], nv_[2];
-    ld2(W + idx0, A[0], A[1]);
-    ld2(W + fsc + idx0, B[0], B[1]);
+    cplx<T>* Wuv = CL ? W + fsc : W;
+    cplx<T> A[2], B[2], U[2], C[2], S[2], nu_[2], nv_[2], o[2], ox[2], oy[2];
+    ld2(Wuv + idx0, A[0], A[1]);
+    ld2(Wuv + fsc + idx0, B[0], B[1]);
+    if (CL) ld2(W + idx0, S[0], S[1]);
     ld2(u0 + idx0, U[0], U[1]);
     if (STAGE > 0) ld2(acc + idx0, C[0], C[1]);
     uint32_t i = idx0 / (uint32_t)nh;
@@ -109,19 +176,27 @@ __global__ void __launch_bounds__(kBlock) k_post2d(cplx<T>* __restrict__ W,
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
         Mode2<T> m = mode2<T>((int)i, (int)j, n);
-        // Basdevant 2D nonlinear term: kx ky FFT(v^2-u^2) + (kx^2-ky^2) FFT(uv)
+        // Basdevant 2D nonlinear term: kx ky FFT(v^2-u^2) + (kx^2-ky^2) FFT(uv), plus the
+        // transformed closure term when one is attached
         cplx<T> N = mk<T>(0, 0);
         if (m.keep) N = axpy(m.kx * m.ky, A[e], scl(m.kx * m.kx - m.ky * m.ky, B[e]));
+        if (CL && m.keep) N = add(N, S[e]);
         IFac<T> f = if_factors(tab, nh, m.akx, m.ky_i, -1, m.k2, p);
         cplx<T> nxt = lawson_stage<T, STAGE>(p.dt, f, N, U[e], C[e]);
         if (STAGE == 3) U[e] = nxt;
         velocity2(m, nxt, p.scale, nu_[e], nv_[e]);
+        if (CL) omega_set(m, nxt, p.scale, o[e], ox[e], oy[e]);
         if (++j == (uint32_t)nh) { j = 0; ++i; }
     }
     if (STAGE == 3) st2(u0 + idx0, U[0], U[1]);
     else st2(acc + idx0, C[0], C[1]);
-    st2(W + idx0, nu_[0], nu_[1]);
-    st2(W + fsc + idx0, nv_[0], nv_[1]);
+    st2(Wuv + idx0, nu_[0], nu_[1]);
+    st2(Wuv + fsc + idx0, nv_[0], nv_[1]);
+    if (CL) {
+        st2(W + 3 * (size_t)fsc + idx0, o[0], o[1]);
+        st2(W + 4 * (size_t)fsc + idx0, ox[0], ox[1]);
+        st2(W + 5 * (size_t)fsc + idx0, oy[0], oy[1]);
+    }
 }
 
 // --------------------------------------------------------------------------------------- 3D

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "spectral_b200.h"
+#include "closure.cuh"
 #include "fused2d.h"
 #include "pointwise.cuh"
 #include "reduce.cuh"
@@ -78,6 +79,11 @@ struct sp_solver {
     // cuFFT
     cufftHandle plan_inv = 0, plan_fwd = 0, plan_c2r1 = 0;
     bool have_inv = false, have_fwd = false, have_c2r1 = false;
+    // learned closure (coarse 2D runs): work slots [S, u, v, omega, omega_x, omega_y], a batch-5
+    // inverse plan over slots 1..5 and a batch-3 forward plan over slots 0..2
+    sp_closure* closure = nullptr;
+    cufftHandle plan_cl_inv = 0, plan_cl_fwd = 0;
+    bool have_cl = false;
     size_t ws_bytes = 0;
     // physics and the host copy of the device parameter block
     double nu = 0, alpha = 0, drag_k2 = 1e30, klo = 0, khi = 0, amp = 0;
@@ -103,6 +109,7 @@ struct sp_solver {
     void* tw_dev() const { return (char*)aux + off_tw; }
     void* u0t_dev() const { return (char*)W + off_u0t; }
     bool fused() const { return fft_mode == SP_FFT_FUSED; }
+    bool cl() const { return closure != nullptr; }
 };
 
 namespace {
@@ -234,6 +241,7 @@ int exec_r2c(sp_solver* s, cufftHandle plan, void* field, cudaStream_t st) {
 size_t field_bytes(const sp_solver* s) { return (size_t)s->fsc * 2 * s->rsize; }
 
 int fft_inverse(sp_solver* s, cudaStream_t st) {
+    if (s->cl()) return exec_c2r(s, s->plan_cl_inv, (char*)s->W + field_bytes(s), st);
     if (s->fft_mode == SP_FFT_CUFFT) return exec_c2r(s, s->plan_inv, s->W, st);
     for (int i = 0; i < s->ninv; ++i) {
         int r = exec_c2r(s, s->plan_inv, (char*)s->W + i * field_bytes(s), st);
@@ -243,6 +251,7 @@ int fft_inverse(sp_solver* s, cudaStream_t st) {
 }
 
 int fft_forward(sp_solver* s, cudaStream_t st) {
+    if (s->cl()) return exec_r2c(s, s->plan_cl_fwd, s->W, st);
     if (s->fft_mode == SP_FFT_CUFFT) return exec_r2c(s, s->plan_fwd, s->W, st);
     for (int i = 0; i < s->nfwd; ++i) {
         int r = exec_r2c(s, s->plan_fwd, (char*)s->W + i * field_bytes(s), st);
@@ -258,7 +267,9 @@ int launch_pre(sp_solver* s, cudaStream_t st) {
     auto* W = (cplx<T>*)s->W;
     auto* P = (const StepParams<T>*)s->params_dev();
     unsigned g = grid_for(s->fsc / 2, kBlock);
-    if (s->dim == 2) k_pre2d<T><<<g, kBlock, 0, st>>>(u0, W, s->n, s->nh, s->fsc, P);
+    if (s->dim == 2 && s->cl())
+        k_pre2d<T, true><<<g, kBlock, 0, st>>>(u0, W, s->n, s->nh, s->fsc, P);
+    else if (s->dim == 2) k_pre2d<T><<<g, kBlock, 0, st>>>(u0, W, s->n, s->nh, s->fsc, P);
     else if (s->form == SP_FORM_ROTATIONAL)
         k_pre3d<T, true><<<g, kBlock, 0, st>>>(u0, W, s->n, s->nh, s->fsc, P);
     else k_pre3d<T, false><<<g, kBlock, 0, st>>>(u0, W, s->n, s->nh, s->fsc, P);
@@ -271,6 +282,12 @@ template <typename T>
 int launch_phys(sp_solver* s, cudaStream_t st) {
     auto* R = (T*)s->W;
     unsigned g = grid_for(s->fsr / 4, kBlock);
+    if (s->cl()) {
+        // products and the closure term in one pass over the coarse field
+        SP_CUDA(sp::closure::les_phase(s->closure, (float*)s->W, s->n, s->fsr, st));
+        s->launches += 1;
+        return SP_OK;
+    }
     if (s->dim == 2) k_phys2d<T><<<g, kBlock, 0, st>>>(R, s->fsr);
     else if (s->form == SP_FORM_ROTATIONAL) k_phys3d_rot<T><<<g, kBlock, 0, st>>>(R, s->fsr);
     else k_phys3d_basd<T><<<g, kBlock, 0, st>>>(R, s->fsr);
@@ -287,7 +304,9 @@ void post_stage(sp_solver* s, cudaStream_t st) {
     auto* tab = (const T*)s->tab_dev();
     auto* P = (const StepParams<T>*)s->params_dev();
     unsigned g = grid_for(s->fsc / 2, kBlock);
-    if (s->dim == 2)
+    if (s->dim == 2 && s->cl())
+        k_post2d<T, STAGE, true><<<g, kBlock, 0, st>>>(W, u0, acc, tab, P, s->n, s->nh, s->fsc);
+    else if (s->dim == 2)
         k_post2d<T, STAGE><<<g, kBlock, 0, st>>>(W, u0, acc, tab, P, s->n, s->nh, s->fsc);
     else if (s->form == SP_FORM_ROTATIONAL)
         k_post3d<T, true, STAGE><<<g, kBlock, 0, st>>>(W, u0, acc, tab, P, s->n, s->nh, s->fsc);
@@ -493,6 +512,10 @@ void sp_destroy(sp_solver* s) {
     if (s->have_inv) cufftDestroy(s->plan_inv);
     if (s->have_fwd) cufftDestroy(s->plan_fwd);
     if (s->have_c2r1) cufftDestroy(s->plan_c2r1);
+    if (s->have_cl) {
+        cufftDestroy(s->plan_cl_inv);
+        cufftDestroy(s->plan_cl_fwd);
+    }
     delete s;
 }
 
@@ -528,6 +551,10 @@ int sp_bind(sp_solver* s, void* u0, void* acc, void* work, void* aux, void* fft_
         SP_CUFFT(cufftSetWorkArea(s->plan_inv, fft_workspace));
         SP_CUFFT(cufftSetWorkArea(s->plan_fwd, fft_workspace));
         if (s->have_c2r1) SP_CUFFT(cufftSetWorkArea(s->plan_c2r1, fft_workspace));
+        if (s->have_cl) {
+            SP_CUFFT(cufftSetWorkArea(s->plan_cl_inv, fft_workspace));
+            SP_CUFFT(cufftSetWorkArea(s->plan_cl_fwd, fft_workspace));
+        }
     }
     s->bound = true;
     s->tab_valid = false;
@@ -775,6 +802,74 @@ int sp_spectrum(sp_solver* s, const void* state, double* out, int nshell, void* 
                             cudaMemcpyDeviceToHost, st));
     SP_CUDA(cudaStreamSynchronize(st));
     return SP_OK;
+}
+
+int sp_attach_closure(sp_solver* s, sp_closure* c) {
+    if (!s) return SP_ERR_ARG;
+    if (s->bound) return fail(s, SP_ERR_STATE, "sp_attach_closure", "attach before sp_bind");
+    if (!c) return fail(s, SP_ERR_ARG, "sp_attach_closure", "null closure");
+    if (s->closure) return fail(s, SP_ERR_STATE, "sp_attach_closure", "a closure is attached already");
+    if (s->dim != 2 || s->fp64 || s->fft_mode != SP_FFT_CUFFT)
+        return fail(s, SP_ERR_UNSUPPORTED, "sp_attach_closure",
+                    "the closure runs on 2D fp32 solvers with batched cuFFT plans");
+    if (sp::closure::grid_n(c) != s->n)
+        return fail(s, SP_ERR_ARG, "sp_attach_closure", "closure and solver grids differ");
+    size_t ws_inv = 0, ws_fwd = 0;
+    int r = make_plan(s, true, 5, &s->plan_cl_inv, &ws_inv);
+    if (r) return r;
+    r = make_plan(s, false, 3, &s->plan_cl_fwd, &ws_fwd);
+    if (r) {
+        cufftDestroy(s->plan_cl_inv);
+        return r;
+    }
+    s->have_cl = true;
+    s->closure = c;
+    s->ninv = 5;
+    s->nfwd = 3;
+    s->nwork = 6;
+    s->work_bytes = (size_t)s->nwork * field_bytes(s);
+    if (ws_inv > s->ws_bytes) s->ws_bytes = ws_inv;
+    if (ws_fwd > s->ws_bytes) s->ws_bytes = ws_fwd;
+    return SP_OK;
+}
+
+int sp_nonlinear(sp_solver* s, const void* state, void* out, void* stream) {
+    SP_CHECK_BOUND(s);
+    if (!state || !out) return fail(s, SP_ERR_ARG, "sp_nonlinear", "null pointer");
+    if (s->dim != 2 || s->fft_mode != SP_FFT_CUFFT)
+        return fail(s, SP_ERR_UNSUPPORTED, "sp_nonlinear", "2D solvers with batched cuFFT plans only");
+    auto st = (cudaStream_t)stream;
+    if (!s->params_valid) {
+        int r = upload_params(s, s->tab_valid ? s->tab_dt : 0.0, st);
+        if (r) return r;
+    }
+    unsigned g = grid_for(s->fsc / 2, kBlock);
+    int r;
+    if (s->fp64) {
+        k_nl_pre2d<double><<<g, kBlock, 0, st>>>((const cplx<double>*)state, (cplx<double>*)s->W,
+                                                 s->n, s->nh, s->fsc,
+                                                 (const StepParams<double>*)s->params_dev());
+    } else {
+        k_nl_pre2d<float><<<g, kBlock, 0, st>>>((const cplx<float>*)state, (cplx<float>*)s->W, s->n,
+                                                s->nh, s->fsc,
+                                                (const StepParams<float>*)s->params_dev());
+    }
+    SP_CUDA(cudaGetLastError());
+    if ((r = exec_c2r(s, s->plan_inv, s->W, st))) return r;
+    if (s->fp64) k_phys2d<double><<<grid_for(s->fsr / 4, kBlock), kBlock, 0, st>>>((double*)s->W, s->fsr);
+    else k_phys2d<float><<<grid_for(s->fsr / 4, kBlock), kBlock, 0, st>>>((float*)s->W, s->fsr);
+    SP_CUDA(cudaGetLastError());
+    if ((r = exec_r2c(s, s->plan_fwd, s->W, st))) return r;
+    if (s->fp64)
+        k_nl_post2d<double><<<g, kBlock, 0, st>>>((const cplx<double>*)s->W, (cplx<double>*)out,
+                                                  s->n, s->nh, s->fsc);
+    else
+        k_nl_post2d<float><<<g, kBlock, 0, st>>>((const cplx<float>*)s->W, (cplx<float>*)out, s->n,
+                                                 s->nh, s->fsc);
+    SP_CUDA(cudaGetLastError());
+    s->launches += 3;
+    // the work array held the next stage's inputs: rebuild them from the state
+    return run_pre(s, st);
 }
 
 }  // extern "C"

@@ -71,6 +71,7 @@ class B200Solver(SpectralSolver):
             raise _lib.EngineError(f"sp_create failed ({_lib.STATUS_NAMES.get(status.value)}): {msg}")
         self._h = h
         self._finalizer = weakref.finalize(self, lib.sp_destroy, ctypes.c_void_p(h))
+        self._before_bind(h)
         sizes = (ctypes.c_int64 * _lib.SZ_COUNT)()
         self._check(lib.sp_query_sizes(h, sizes, _lib.SZ_COUNT), "sp_query_sizes")
         self.sizes = list(sizes)
@@ -105,6 +106,9 @@ class B200Solver(SpectralSolver):
 
     def _check(self, status: int, what: str) -> None:
         _lib.check(self.lib, self._h, status, what)
+
+    def _before_bind(self, h: int) -> None:
+        """Hook between sp_create and sp_query_sizes / sp_bind (layout-changing attachments)."""
 
     def _stream(self) -> ctypes.c_void_p:
         return ctypes.c_void_p(self.torch.cuda.current_stream(self.device).cuda_stream)

@@ -93,6 +93,13 @@ def main() -> None:
     # spectral filter used by the closure pipeline (validation.py:25-35)
     out["pad_tgv2d_16_to_32"] = pad_spectrum(initial.to_spectral(initial.taylor_green_2d(16), 2),
                                              32, 2)
+    rng = np.random.default_rng(7)
+    for n, n_to, dim in ((32, 16, 2), (16, 24, 2), (24, 24, 2), (16, 8, 3), (8, 12, 3)):
+        shp = (n,) * (dim - 1) + (n // 2 + 1,)
+        a = rng.normal(size=shp) + 1j * rng.normal(size=shp)
+        key = f"pad_rand{dim}d_{n}_to_{n_to}"
+        out[key + "_in"] = a
+        out[key] = pad_spectrum(a, n_to, dim)
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT} ({OUT.stat().st_size / 1024:.0f} KiB, {len(out)} arrays)")
 
