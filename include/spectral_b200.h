@@ -261,6 +261,15 @@ int sp_closure_get_grad(sp_closure* c, float* host);
  * predictions with S * omega > 0 (local enstrophy backscatter) at inference. */
 int sp_closure_set_scales(sp_closure* c, const float* inscale3, float outscale, int clip);
 int sp_closure_get_scales(const sp_closure* c, float* out5);
+/* Per-shell gains g(k) of the closure term in an attached solver's step (N += g(round|k|) S);
+ * nshell = floor(sqrt(2) n/2 + 1/2) + 1 entries (sp_closure_shell_count), all 1 at creation. */
+int sp_closure_set_shell_gain(sp_closure* c, const float* host, int nshell);
+int sp_closure_shell_count(const sp_closure* c);
+/* every_stage != 0 (the default): an attached solver evaluates the network at all four RK
+ * stages; 0: at the first stage of each step only, its transformed term held for the other
+ * three (which then run the plain two-field transforms).  Takes effect at the next step
+ * (re-capture the step graph with sp_set_graph after changing it). */
+int sp_closure_set_update(sp_closure* c, int every_stage);
 /* Adam with linear warm-up over `warmup` steps and cosine decay to lr_min at total_steps. */
 int sp_closure_set_adam(sp_closure* c, double lr, double lr_min, double beta1, double beta2,
                         double eps, int total_steps, int warmup);

@@ -81,6 +81,9 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_closure_set_scales": (_i, [_vp, _vp, _f, _i]),
     "sp_closure_get_scales": (_i, [_vp, _vp]),
     "sp_closure_set_adam": (_i, [_vp, _d, _d, _d, _d, _d, _i, _i]),
+    "sp_closure_set_shell_gain": (_i, [_vp, _vp, _i]),
+    "sp_closure_shell_count": (_i, [_vp]),
+    "sp_closure_set_update": (_i, [_vp, _i]),
     "sp_closure_bank_load": (_i, [_vp, _vp, _i]),
     "sp_closure_add_snapshot": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "sp_closure_bank_read": (_i, [_vp, _i, _vp]),

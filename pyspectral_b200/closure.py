@@ -80,6 +80,9 @@ class ClosureNet:
         self.inscale = np.ones(3, np.float32)
         self.outscale = 1.0
         self.clip = False
+        self.nshell = int(lib.sp_closure_shell_count(h))
+        self.shell_gain = np.ones(self.nshell, np.float32)
+        self.every_stage = True
 
     # ------------------------------------------------------------------ plumbing
     @property
@@ -122,6 +125,21 @@ class ClosureNet:
         self._check(self.lib.sp_closure_set_scales(self._h, _fptr(a), float(outscale), int(clip)),
                     "sp_closure_set_scales")
         self.inscale, self.outscale, self.clip = a.copy(), float(outscale), bool(clip)
+
+    def set_shell_gain(self, gain: Any) -> None:
+        """Per-shell gains g(k) applied to the closure term in an attached solver's step."""
+        g = np.ascontiguousarray(gain, dtype=np.float32)
+        if g.shape != (self.nshell,):
+            raise ValueError(f"expected {self.nshell} shell gains, got {g.shape}")
+        self._check(self.lib.sp_closure_set_shell_gain(self._h, _fptr(g), self.nshell),
+                    "sp_closure_set_shell_gain")
+        self.shell_gain = g.copy()
+
+    def set_update(self, every_stage: bool) -> None:
+        """Network evaluated at every RK stage, or at the first stage of each step only."""
+        self._check(self.lib.sp_closure_set_update(self._h, int(bool(every_stage))),
+                    "sp_closure_set_update")
+        self.every_stage = bool(every_stage)
 
     def fit_scales(self, max_entries: int = 64, clip: bool = False) -> None:
         """Unit-variance inputs and target from the standard deviations over (part of) the bank."""
@@ -221,7 +239,7 @@ class ClosureNet:
     # ------------------------------------------------------------------ files
     def save(self, path: str | Path) -> None:
         np.savez(path, params=self.params(), inscale=self.inscale, outscale=self.outscale,
-                 clip=self.clip, n=self.n)
+                 clip=self.clip, n=self.n, shell_gain=self.shell_gain)
 
     def load(self, path: str | Path) -> None:
         z = np.load(path)
@@ -229,6 +247,8 @@ class ClosureNet:
             raise ValueError(f"closure file is for n={int(z['n'])}, this network has n={self.n}")
         self.set_params(z["params"])
         self.set_scales(z["inscale"], float(z["outscale"]), bool(z["clip"]))
+        if "shell_gain" in z.files:
+            self.set_shell_gain(z["shell_gain"])
 
 
 # ---------------------------------------------------------------------- spectral helpers
@@ -288,18 +308,31 @@ class SnapshotPipeline:
 class ClosureSolver(B200Solver):
     """Coarse 2D fp32 solver whose RK stages add the network's subgrid term to the nonlinear
     term: stage = batch-5 inverse FFT (u, v, omega, omega_x, omega_y) -> products + network
-    (one persistent tcgen05 kernel) -> batch-3 forward FFT (S, products) -> Lawson update."""
+    (one persistent tcgen05 kernel) -> batch-3 forward FFT (S, products) -> Lawson update.
+    ``every_stage=False`` evaluates the network at the first stage of each step only and holds
+    its term for the other three stages, which run the plain two-field transforms."""
 
     variant = "closure-les-graph"
     dims: ClassVar[tuple[int, ...]] = (2,)
 
-    def __init__(self, cfg: Config, net: ClosureNet) -> None:
+    def __init__(self, cfg: Config, net: ClosureNet, every_stage: bool = True) -> None:
         if cfg.dim != 2 or cfg.is_fp64:
             raise BackendUnavailable("closure: 2D fp32 runs only")
         if cfg.n != net.n:
             raise ValueError(f"closure network is for n={net.n}, run has n={cfg.n}")
         self.net = net
+        self.every_stage = bool(every_stage)
+        self._mode: bool | None = None  # update mode the step graph was captured with
         super().__init__(cfg)
+
+    def _step(self, dt: float) -> None:
+        if self._mode != self.every_stage or self.net.every_stage != self.every_stage:
+            # the closure object is shared: set its mode and re-capture this solver's graph
+            self.net.set_update(self.every_stage)
+            self._check(self.lib.sp_set_graph(self._h, 0), "sp_set_graph")
+            self._check(self.lib.sp_set_graph(self._h, int(self.use_graph)), "sp_set_graph")
+            self._mode = self.every_stage
+        super()._step(dt)
 
     def _before_bind(self, h: int) -> None:
         _lib.check(self.lib, h, self.lib.sp_attach_closure(h, ctypes.c_void_p(self.net.handle)),

@@ -38,18 +38,20 @@ namespace {
 constexpr uint32_t kWait = 1u << 22;  // mbarrier polls before a wait gives up
 
 // ------------------------------------------------------------------------ device helpers
-// GELU, tanh form (Hendrycks and Gimpel), and its derivative.
-__device__ __forceinline__ float gelu(float z) {
-    const float c0 = 0.7978845608028654f, c1 = 0.044715f;
-    const float t = tanhf(c0 * z * (1.f + c1 * z * z));
-    return 0.5f * z * (1.f + t);
+// GELU, tanh form (Hendrycks and Gimpel): 0.5 z (1 + tanh u) with u = c0 (z + c1 z^3), written
+// as z s with the logistic factor s = (1 + tanh u) / 2 = 1 / (1 + exp(-2u)); its derivative is
+// s + 2 z s (1 - s) c0 (1 + 3 c1 z^2).
+constexpr float kGc0 = 0.7978845608028654f, kGc1 = 0.044715f;
+__device__ __forceinline__ float gelu_s(float z) {
+    // the exponent is capped so that 1 + exp stays finite (s is 0 to fp32 precision there)
+    const float a = fminf(-2.f * kGc0 * z * (1.f + kGc1 * z * z), 80.f);
+    return __fdividef(1.f, 1.f + __expf(a));
 }
+__device__ __forceinline__ float gelu(float z) { return z * gelu_s(z); }
 __device__ __forceinline__ float gelu_d(float z, float& g) {
-    const float c0 = 0.7978845608028654f, c1 = 0.044715f;
-    const float z2 = z * z;
-    const float t = tanhf(c0 * z * (1.f + c1 * z2));
-    g = 0.5f * z * (1.f + t);
-    return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * c0 * (1.f + 3.f * c1 * z2);
+    const float s = gelu_s(z);
+    g = z * s;
+    return s + 2.f * z * s * (1.f - s) * kGc0 * (1.f + 3.f * kGc1 * z * z);
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
@@ -110,10 +112,67 @@ __device__ __forceinline__ void stage_stencil(float* sSt, const float* f0, size_
     }
 }
 
-// Feature row of point p (75 stencil values, the constant one, zero padding) into the X tile.
+// Inference staging: the scaled stencil rounded to bf16 once (the value X receives).
+template <int THREADS>
+__device__ __forceinline__ void stage_stencil_bf16(__nv_bfloat16* sSt, const float* f0,
+                                                   size_t fstride, int rstride, int n, int row,
+                                                   int y0, const Consts& cc) {
+    constexpr int kPer = (kStencil + THREADS - 1) / THREADS;
+    float v[kPer];
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {  // all loads first
+        const int e = threadIdx.x + i * THREADS;
+        if (e < kStencil) {
+            const int f = e / (5 * kSpan);
+            const int r = (e / kSpan) % 5;
+            const int c = e % kSpan;
+            const int xr = (row + r - kHalo) & (n - 1);
+            const int yc = (y0 + c - kHalo) & (n - 1);
+            v[i] = f0[(size_t)f * fstride + (size_t)xr * rstride + yc];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int e = threadIdx.x + i * THREADS;
+        if (e < kStencil) {
+            const int f = e / (5 * kSpan);
+            const float sc = f == 0 ? cc.inscale[0] : (f == 1 ? cc.inscale[1] : cc.inscale[2]);
+            sSt[e] = __float2bfloat16_rn(v[i] * sc);
+        }
+    }
+}
+
+template <int G0, int G1>
+__device__ __forceinline__ void build_x_bf16(unsigned char* sX, const __nv_bfloat16* sSt, int p) {
+    const unsigned short* src = reinterpret_cast<const unsigned short*>(sSt);
+#pragma unroll
+    for (int g = G0; g < G1; ++g) {
+        uint32_t h[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int f = 8 * g + i;
+            if (f < kIn) {
+                const int fld = f / 25, rr = (f % 25) / 5, cc = f % 5;
+                h[i] = src[fld * 5 * kSpan + rr * kSpan + p + cc];
+            } else {
+                h[i] = f == kBiasIn ? 0x3F80u : 0u;  // bf16 1.0
+            }
+        }
+        uint4 q;
+        q.x = h[0] | (h[1] << 16);
+        q.y = h[2] | (h[3] << 16);
+        q.z = h[4] | (h[5] << 16);
+        q.w = h[6] | (h[7] << 16);
+        *reinterpret_cast<uint4*>(sX + tc::core_offset(p, 8 * g, kK)) = q;
+    }
+}
+
+// Feature groups [G0, G1) (8 inputs each: 75 stencil values, the constant one, zero padding) of
+// point p into the X tile.
+template <int G0 = 0, int G1 = kK / 8>
 __device__ __forceinline__ void build_x(unsigned char* sX, const float* sSt, int p) {
 #pragma unroll
-    for (int g = 0; g < kK / 8; ++g) {
+    for (int g = G0; g < G1; ++g) {
         float v[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -140,13 +199,32 @@ __device__ __forceinline__ void init_hidden_bias(unsigned char* sHt, int p) {
     st_row8(sHt, p, 72, kK, v);
 }
 
-// Copies the three bf16 weight matrices [64][80] (row-major) into core-layout tiles.
+// Element index, in the bf16 weight copy, of parameter j < 3 * 5120: the three [64][80]
+// matrices are kept in the core-matrix layout their shared-memory operand tiles use, so that
+// staging them is a contiguous copy.
+__host__ __device__ __forceinline__ int wb_index(int j) {
+    const int l = j / kWsz, e = j % kWsz;
+    return l * kWsz + (int)(tc::core_offset(e / kK, e % kK, kK) / 2);
+}
+
+// Copies the three bf16 weight tiles (already in core layout) into shared memory; every
+// thread's loads are issued before its stores.
+template <int THREADS>
 __device__ __forceinline__ void stage_weights(unsigned char* sW, const __nv_bfloat16* wb) {
+    constexpr int kQ = kLayers * kWsz / 8;  // 16-byte chunks
+    constexpr int kPer = (kQ + THREADS - 1) / THREADS;
     const uint4* src = reinterpret_cast<const uint4*>(wb);
-    for (int q = threadIdx.x; q < kLayers * kWsz / 8; q += blockDim.x) {
-        const int l = q / (kWsz / 8), e = (q % (kWsz / 8)) * 8;
-        const int r = e / kK, c = e % kK;
-        *reinterpret_cast<uint4*>(sW + l * kWsz * 2 + tc::core_offset(r, c, kK)) = src[q];
+    uint4* dst = reinterpret_cast<uint4*>(sW);
+    uint4 v[kPer];
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int q = threadIdx.x + i * THREADS;
+        if (q < kQ) v[i] = src[q];
+    }
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int q = threadIdx.x + i * THREADS;
+        if (q < kQ) dst[q] = v[i];
     }
 }
 
@@ -236,7 +314,7 @@ __global__ void __launch_bounds__(128, 1)
     const Consts cc = *ccp;
     const int64_t step = step_override >= 0 ? step_override : (int64_t)*step_dev;
 
-    stage_weights(sW, wb);
+    stage_weights<128>(sW, wb);
     if (t < kK) {
         sW4[t] = params[kLayers * kWsz + t];
         sDW4[t] = 0.f;
@@ -448,30 +526,50 @@ __global__ void k_adam(float* __restrict__ params, float* __restrict__ m, float*
     const float vh = vj / (1.f - powf(cfg.b2, (float)t));
     const float p = params[j] - lr * mh / (sqrtf(vh) + cfg.eps);
     params[j] = p;
-    if (j < kLayers * kWsz) wb[j] = __float2bfloat16_rn(p);
+    if (j < kLayers * kWsz) wb[wb_index(j)] = __float2bfloat16_rn(p);
 }
 
 __global__ void k_to_bf16(const float* __restrict__ params, __nv_bfloat16* __restrict__ wb) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < kLayers * kWsz) wb[j] = __float2bfloat16_rn(params[j]);
+    if (j < kLayers * kWsz) wb[wb_index(j)] = __float2bfloat16_rn(params[j]);
 }
 
 // ------------------------------------------------------------------------ inference kernel
+// Eight warps per CTA: warps w and w + 4 serve the TMEM lanes (points) 32 (w % 4) .. + 31 and
+// split the 64 hidden columns in halves; X and the hidden activations share one operand buffer
+// (each layer's epilogue runs after the MMA that read the buffer has completed), so three CTAs
+// fit on an SM.
 struct InferSmem {
-    static constexpr int W = 0;
-    static constexpr int X = W + kLayers * kWsz * 2;
-    static constexpr int H = X + kTile * kK * 2;
-    static constexpr int ST = H + kTile * kK * 2;
-    static constexpr int W4 = ST + kStencil * 4;
-    static constexpr int BYTES = W4 + kK * 4;
+    static constexpr int W = 0;                                  // 3 x [64 x 80] bf16
+    static constexpr int A = W + kLayers * kWsz * 2;             // X, then H1, H2 [128 x 80]
+    static constexpr int ST = A + kTile * kK * 2;                // stencil, bf16
+    static constexpr int W4 = ST + ((kStencil * 2 + 15) / 16) * 16;  // w4 fp32 [80]
+    static constexpr int YP = W4 + kK * 4;                       // upper-half output partials
+    static constexpr int BYTES = YP + kTile * 4;
 };
 constexpr uint32_t kInferCols = 64;
+// four CTAs per SM: one wave of 128-point tiles covers 256^2 on 148 SMs
+constexpr int kInferThreads = 256, kInferCtasPerSm = 4;
+
+// Hidden epilogue of one column half: 32 columns of row p -> GELU -> bf16 operand buffer.
+__device__ __forceinline__ void epi_half(uint32_t tb, int quad, int ch, unsigned char* sA, int p) {
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+        float z[16];
+        tc::tmem_ld16(tc::tmem_at(tb, 32 * quad, 32 * ch + 16 * h), z);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) z[i] = gelu(z[i]);
+        st_row8(sA, p, 32 * ch + 16 * h, kK, z);
+        st_row8(sA, p, 32 * ch + 16 * h + 8, kK, z + 8);
+    }
+}
 
 // Closure term at every point of an n x n field, one 128-point row segment per tile.
 // fields: omega, d omega/dx, d omega/dy at f0 + k * fstride (row stride rstride); out gets
 // outscale * network (row stride out_rstride).  With uv set, the Basdevant products of the
 // velocity pair at uv, uv + uv_stride (same row stride) are formed in place as well.
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kInferThreads, kInferCtasPerSm)
     k_infer(const float* __restrict__ f0, size_t fstride, int rstride, int n,
             const __nv_bfloat16* __restrict__ wb, const float* __restrict__ params,
             const Consts* __restrict__ ccp, float* __restrict__ out, int out_rstride,
@@ -480,16 +578,17 @@ __global__ void __launch_bounds__(128)
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tslot;
     unsigned char* sW = smem + InferSmem::W;
-    unsigned char* sX = smem + InferSmem::X;
-    unsigned char* sH = smem + InferSmem::H;
-    float* sSt = reinterpret_cast<float*>(smem + InferSmem::ST);
+    unsigned char* sA = smem + InferSmem::A;
+    __nv_bfloat16* sSt = reinterpret_cast<__nv_bfloat16*>(smem + InferSmem::ST);
     float* sW4 = reinterpret_cast<float*>(smem + InferSmem::W4);
-    const int t = threadIdx.x, warp = t >> 5;
+    float* sYP = reinterpret_cast<float*>(smem + InferSmem::YP);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int quad = warp & 3, ch = warp >> 2;  // TMEM lane quadrant, hidden column half
+    const int p = 32 * quad + lane;             // this thread's point in the tile
     const Consts cc = *ccp;
 
-    stage_weights(sW, wb);
+    stage_weights<kInferThreads>(sW, wb);
     if (t < kK) sW4[t] = params[kLayers * kWsz + t];
-    init_hidden_bias(sH, t);
     if (t == 0) {
         tc::mbar_init(&bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -497,7 +596,7 @@ __global__ void __launch_bounds__(128)
     if (warp == 0) tc::tmem_alloc(&tslot, kInferCols);
     sync_for_mma();
     const uint32_t tb = tslot;
-    const uint32_t aX = tc::smem_u32(sX), aH = tc::smem_u32(sH), aW = tc::smem_u32(sW);
+    const uint32_t aA = tc::smem_u32(sA), aW = tc::smem_u32(sW);
 
     uint32_t phase = 0;
     bool ok = true;
@@ -505,51 +604,57 @@ __global__ void __launch_bounds__(128)
     const int ntiles = n * segs;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int row = tile / segs, y0 = (tile % segs) * kTile;
-        stage_stencil(sSt, f0, fstride, rstride, n, row, y0, cc);
-        if (uv) {
-            float* pu = uv + (size_t)row * rstride + y0 + t;
+        stage_stencil_bf16<kInferThreads>(sSt, f0, fstride, rstride, n, row, y0, cc);
+        if (uv && ch == 0) {
+            float* pu = uv + (size_t)row * rstride + y0 + p;
             const float u = pu[0], v = pu[uv_stride];
             pu[0] = (v - u) * (v + u);
             pu[uv_stride] = u * v;
         }
         __syncthreads();
-        build_x(sX, sSt, t);
+        if (ch == 0) build_x_bf16<0, kK / 16>(sA, sSt, p);
+        else build_x_bf16<kK / 16, kK / 8>(sA, sSt, p);
         sync_for_mma();
         if (t == 0) {
-            issue(tb, aX, 0, kK, aW, 0, kK, 128, kH, kK / 16, false);
+            issue(tb, aA, 0, kK, aW, 0, kK, 128, kH, kK / 16, false);
             tc::mma_commit(&bar);
         }
         if (!(ok = wait_mma(&bar, phase))) break;
-        epi_forward(tb, 0, sH, t, warp);
+        epi_half(tb, quad, ch, sA, p);
+        if (ch == 1) init_hidden_bias(sA, p);  // X's inputs 64..79 become the bias column
         sync_for_mma();
         if (t == 0) {
-            issue(tb, aH, 0, kK, aW + kWsz * 2, 0, kK, 128, kH, kK / 16, false);
+            issue(tb, aA, 0, kK, aW + kWsz * 2, 0, kK, 128, kH, kK / 16, false);
             tc::mma_commit(&bar);
         }
         if (!(ok = wait_mma(&bar, phase))) break;
-        epi_forward(tb, 0, sH, t, warp);
+        epi_half(tb, quad, ch, sA, p);
         sync_for_mma();
         if (t == 0) {
-            issue(tb, aH, 0, kK, aW + 2 * kWsz * 2, 0, kK, 128, kH, kK / 16, false);
+            issue(tb, aA, 0, kK, aW + 2 * kWsz * 2, 0, kK, 128, kH, kK / 16, false);
             tc::mma_commit(&bar);
         }
         if (!(ok = wait_mma(&bar, phase))) break;
-        float y = sW4[kBiasH];
+        float y = 0.f;
 #pragma unroll 1
-        for (int c = 0; c < kH; c += 8) {
-            float z[8];
-            tc::tmem_ld8(tc::tmem_at(tb, 32 * warp, c), z);
+        for (int h = 0; h < 2; ++h) {
+            float z[16];
+            tc::tmem_ld16(tc::tmem_at(tb, 32 * quad, 32 * ch + 16 * h), z);
             tc::tmem_wait_ld();
 #pragma unroll
-            for (int i = 0; i < 8; ++i) y += gelu(z[i]) * sW4[c + i];
+            for (int i = 0; i < 16; ++i) y += gelu(z[i]) * sW4[32 * ch + 16 * h + i];
         }
-        float S = cc.outscale * y;
-        if (cc.clip) {
-            const float w = f0[(size_t)row * rstride + y0 + t];
-            if (S * w > 0.f) S = 0.f;
+        if (ch == 1) sYP[p] = y;
+        __syncthreads();
+        if (ch == 0) {
+            float S = cc.outscale * (sW4[kBiasH] + y + sYP[p]);
+            if (cc.clip) {
+                const float w = f0[(size_t)row * rstride + y0 + p];
+                if (S * w > 0.f) S = 0.f;
+            }
+            out[(size_t)row * out_rstride + y0 + p] = S;
         }
-        out[(size_t)row * out_rstride + y0 + t] = S;
-        // the next tile's MMA must not overtake this tile's TMEM reads
+        // the next tile's MMA and partials must not overtake this tile's TMEM and sYP reads
         tc::fence_before_sync();
         __syncthreads();
         tc::fence_after_sync();
@@ -649,6 +754,9 @@ struct sp_closure {
     int* step_dev = nullptr;
     int* err = nullptr;
     Consts* consts_dev = nullptr;
+    float* shell_gain = nullptr;  // per-shell gain of the closure term in the coarse step
+    int nshell = 0;
+    int every_stage = 1;  // evaluate the network at every RK stage (1) or at the first only (0)
     Consts consts{};
     AdamCfg adam{1e-3f, 1e-5f, 0.9f, 0.999f, 1e-8f, 20000, 200};
     int64_t host_step = 0;
@@ -726,7 +834,7 @@ int upload_consts(sp_closure* c) {
 
 int infer_grid(const sp_closure* c, int n) {
     const int ntiles = n * (n / kTile);
-    return ntiles < 2 * c->sms ? ntiles : 2 * c->sms;
+    return ntiles < kInferCtasPerSm * c->sms ? ntiles : kInferCtasPerSm * c->sms;
 }
 
 }  // namespace
@@ -736,9 +844,13 @@ namespace closure {
 
 int grid_n(const sp_closure* c) { return c ? c->n : 0; }
 
+const float* shell_gain(const sp_closure* c) { return c->shell_gain; }
+bool every_stage(const sp_closure* c) { return c->every_stage != 0; }
+int shell_count(const sp_closure* c) { return c->nshell; }
+
 cudaError_t les_phase(const sp_closure* c, float* R, int n, uint32_t fsr, cudaStream_t st) {
     const int rs = n + 2;
-    k_infer<<<infer_grid(c, n), 128, InferSmem::BYTES, st>>>(
+    k_infer<<<infer_grid(c, n), kInferThreads, InferSmem::BYTES, st>>>(
         R + 3 * (size_t)fsr, fsr, rs, n, c->wb, c->params, c->consts_dev, R, rs, R + fsr, fsr,
         c->err);
     return cudaGetLastError();
@@ -789,6 +901,8 @@ sp_closure* sp_closure_create(int n, int capacity, int* status) {
                cudaMalloc(&c->err, sizeof(int)) == cudaSuccess &&
                cudaMalloc(&c->consts_dev, sizeof(Consts)) == cudaSuccess &&
                cudaMalloc(&c->spec, 4 * (size_t)c->fsc * sizeof(cplx<float>)) == cudaSuccess;
+    c->nshell = (int)std::floor(std::sqrt(2.0) * (double)(n / 2) + 0.5) + 1;
+    okm = okm && cudaMalloc(&c->shell_gain, c->nshell * sizeof(float)) == cudaSuccess;
     if (!okm) return fail_create("allocation failed");
     bool okz = cudaMemset(c->params, 0, kNParam * sizeof(float)) == cudaSuccess &&
                cudaMemset(c->adam_m, 0, kNParam * sizeof(float)) == cudaSuccess &&
@@ -799,6 +913,12 @@ sp_closure* sp_closure_create(int n, int capacity, int* status) {
                cudaMemset(c->step_dev, 0, sizeof(int)) == cudaSuccess &&
                cudaMemset(c->err, 0, sizeof(int)) == cudaSuccess;
     if (!okz) return fail_create("initialisation failed");
+    {
+        std::vector<float> ones(c->nshell, 1.f);
+        if (cudaMemcpy(c->shell_gain, ones.data(), c->nshell * sizeof(float),
+                       cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail_create("initialisation failed");
+    }
     for (int f = 0; f < 3; ++f) c->consts.inscale[f] = 1.f;
     c->consts.outscale = 1.f;
     c->consts.inv_outscale = 1.f;
@@ -807,7 +927,9 @@ sp_closure* sp_closure_create(int n, int capacity, int* status) {
     if (cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              TrainSmem::BYTES) != cudaSuccess ||
         cudaFuncSetAttribute(k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             InferSmem::BYTES) != cudaSuccess)
+                             InferSmem::BYTES) != cudaSuccess ||
+        cudaFuncSetAttribute(k_infer, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared) != cudaSuccess)
         return fail_create("cudaFuncSetAttribute failed");
     // batch of 4 out-of-place C2R transforms: spectral scratch -> unpadded bank fields
     long long shape[2] = {n, n}, cemb[2] = {n, c->nh}, remb[2] = {n, n};
@@ -834,7 +956,7 @@ void sp_closure_destroy(sp_closure* c) {
     for (void* p : {(void*)c->bank, (void*)c->params, (void*)c->adam_m, (void*)c->adam_v,
                     (void*)c->grad, (void*)c->partials, (void*)c->loss, (void*)c->wb,
                     (void*)c->step_dev, (void*)c->err, (void*)c->consts_dev, (void*)c->spec,
-                    c->plan_ws})
+                    (void*)c->shell_gain, c->plan_ws})
         if (p) cudaFree(p);
     delete c;
 }
@@ -887,6 +1009,20 @@ int sp_closure_get_scales(const sp_closure* c, float* out5) {
     for (int f = 0; f < 3; ++f) out5[f] = c->consts.inscale[f];
     out5[3] = c->consts.outscale;
     out5[4] = (float)c->consts.clip;
+    return SP_OK;
+}
+
+int sp_closure_set_shell_gain(sp_closure* c, const float* host, int nshell) {
+    if (!c || !host || nshell != c->nshell) return SP_ERR_ARG;
+    CL_CUDA(cudaMemcpy(c->shell_gain, host, nshell * sizeof(float), cudaMemcpyHostToDevice));
+    return SP_OK;
+}
+
+int sp_closure_shell_count(const sp_closure* c) { return c ? c->nshell : -1; }
+
+int sp_closure_set_update(sp_closure* c, int every_stage) {
+    if (!c) return SP_ERR_ARG;
+    c->every_stage = every_stage ? 1 : 0;
     return SP_OK;
 }
 
@@ -1023,7 +1159,7 @@ int sp_closure_infer(sp_closure* c, const float* fields, int64_t field_stride, i
         return SP_ERR_ARG;
     auto st = (cudaStream_t)stream;
     const int n = c->n;
-    k_infer<<<infer_grid(c, n), 128, InferSmem::BYTES, st>>>(
+    k_infer<<<infer_grid(c, n), kInferThreads, InferSmem::BYTES, st>>>(
         fields, (size_t)field_stride, row_stride, n, c->wb, c->params, c->consts_dev, out,
         out_row_stride, nullptr, 0, c->err);
     CL_CUDA(cudaGetLastError());

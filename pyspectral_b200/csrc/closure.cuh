@@ -71,5 +71,11 @@ namespace closure {
 // Writes the Basdevant products into the u, v slots in place and the closure term into S.
 cudaError_t les_phase(const sp_closure* c, float* R, int n, uint32_t fsr, cudaStream_t st);
 int grid_n(const sp_closure* c);
+// Per-shell gains (shell = round(|k|), shell_count entries) applied to the closure term.
+const float* shell_gain(const sp_closure* c);
+int shell_count(const sp_closure* c);
+// Whether the network runs at every RK stage or only at the first stage of each step (its term
+// then held for the step's other stages).
+bool every_stage(const sp_closure* c);
 }  // namespace closure
 }  // namespace sp

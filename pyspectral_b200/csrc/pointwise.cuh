@@ -160,7 +160,9 @@ __global__ void __launch_bounds__(kBlock) k_post2d(cplx<T>* __restrict__ W,
                                                    cplx<T>* __restrict__ acc,
                                                    const T* __restrict__ tab,
                                                    const StepParams<T>* __restrict__ P, int n,
-                                                   int nh, uint32_t fsc) {
+                                                   int nh, uint32_t fsc,
+                                                   const float* __restrict__ gain = nullptr,
+                                                   int ngain = 0, int omega_out = 1) {
     uint32_t idx0 = 2u * (blockIdx.x * blockDim.x + threadIdx.x);
     if (idx0 >= fsc) return;
     const StepParams<T> p = *P;
@@ -180,7 +182,11 @@ __global__ void __launch_bounds__(kBlock) k_post2d(cplx<T>* __restrict__ W,
         // transformed closure term when one is attached
         cplx<T> N = mk<T>(0, 0);
         if (m.keep) N = axpy(m.kx * m.ky, A[e], scl(m.kx * m.kx - m.ky * m.ky, B[e]));
-        if (CL && m.keep) N = add(N, S[e]);
+        if (CL && m.keep && m.k2 > (T)0) {  // S is a divergence: no mean
+            int sh = (int)(sqrt(m.k2) + (T)0.5);
+            sh = sh < ngain ? sh : ngain - 1;
+            N = axpy((T)gain[sh], S[e], N);
+        }
         IFac<T> f = if_factors(tab, nh, m.akx, m.ky_i, -1, m.k2, p);
         cplx<T> nxt = lawson_stage<T, STAGE>(p.dt, f, N, U[e], C[e]);
         if (STAGE == 3) U[e] = nxt;
@@ -192,7 +198,7 @@ __global__ void __launch_bounds__(kBlock) k_post2d(cplx<T>* __restrict__ W,
     else st2(acc + idx0, C[0], C[1]);
     st2(Wuv + idx0, nu_[0], nu_[1]);
     st2(Wuv + fsc + idx0, nv_[0], nv_[1]);
-    if (CL) {
+    if (CL && omega_out) {  // the network's inputs, when the next stage evaluates it
         st2(W + 3 * (size_t)fsc + idx0, o[0], o[1]);
         st2(W + 4 * (size_t)fsc + idx0, ox[0], ox[1]);
         st2(W + 5 * (size_t)fsc + idx0, oy[0], oy[1]);

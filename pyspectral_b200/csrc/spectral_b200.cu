@@ -305,7 +305,10 @@ void post_stage(sp_solver* s, cudaStream_t st) {
     auto* P = (const StepParams<T>*)s->params_dev();
     unsigned g = grid_for(s->fsc / 2, kBlock);
     if (s->dim == 2 && s->cl())
-        k_post2d<T, STAGE, true><<<g, kBlock, 0, st>>>(W, u0, acc, tab, P, s->n, s->nh, s->fsc);
+        k_post2d<T, STAGE, true><<<g, kBlock, 0, st>>>(
+            W, u0, acc, tab, P, s->n, s->nh, s->fsc, sp::closure::shell_gain(s->closure),
+            sp::closure::shell_count(s->closure),
+            (STAGE == 3 || sp::closure::every_stage(s->closure)) ? 1 : 0);
     else if (s->dim == 2)
         k_post2d<T, STAGE><<<g, kBlock, 0, st>>>(W, u0, acc, tab, P, s->n, s->nh, s->fsc);
     else if (s->form == SP_FORM_ROTATIONAL)
@@ -350,9 +353,35 @@ int fused_col(sp_solver* s, int stage, cudaStream_t st) {
     return SP_OK;
 }
 
+// Stage of a closure run whose network term is held from the step's first stage: the plain
+// velocity-pair transforms and products on work slots 1-2; slot 0 keeps the transformed term.
+int held_closure_stage(sp_solver* s, cudaStream_t st) {
+    char* Wuv = (char*)s->W + field_bytes(s);
+    int r;
+    if ((r = exec_c2r(s, s->plan_inv, Wuv, st))) return r;
+    k_phys2d<float><<<grid_for(s->fsr / 4, kBlock), kBlock, 0, st>>>((float*)Wuv, s->fsr);
+    SP_CUDA(cudaGetLastError());
+    s->launches += 1;
+    return exec_r2c(s, s->plan_fwd, Wuv, st);
+}
+
 // One IF-RK4 step: 4 x (inverse FFT -> phys -> forward FFT -> post), cupy_cuda.py:163-178;
 // in the fused mode 4 x (row pass -> column pass).
 int run_step(sp_solver* s, cudaStream_t st) {
+    if (s->cl() && !sp::closure::every_stage(s->closure)) {
+        for (int stage = 0; stage < 4; ++stage) {
+            int r;
+            if (stage == 0) {
+                if ((r = fft_inverse(s, st))) return r;
+                if ((r = run_phys(s, st))) return r;
+                if ((r = fft_forward(s, st))) return r;
+            } else if ((r = held_closure_stage(s, st))) {
+                return r;
+            }
+            if ((r = run_post(s, stage, st))) return r;
+        }
+        return SP_OK;
+    }
     if (s->fused()) {
         for (int stage = 0; stage < 4; ++stage) {
             int r;

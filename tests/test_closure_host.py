@@ -135,3 +135,13 @@ def test_snapshot_fields_derivatives():
     np.testing.assert_allclose(f[1], 3 * np.cos(3 * x)[:, None] * np.cos(2 * x)[None, :], atol=1e-11)
     np.testing.assert_allclose(f[2], -2 * np.sin(3 * x)[:, None] * np.sin(2 * x)[None, :], atol=1e-11)
     assert np.all(f[3] == 0)
+
+
+def test_study_config_cutoffs():
+    from pyspectral_b200.closure_les import StudyConfig
+
+    sc = StudyConfig()
+    assert sc.k_check == 85 and sc.n_fine == 2048 and sc.snapshots == 4000
+    assert sc.batch_tiles * 128 == 65536 and sc.train_steps == 20000
+    small = StudyConfig.small()
+    assert small.k_check == 42 and 3 * small.k_check < small.n_coarse <= 3 * (small.k_check + 1)

@@ -234,23 +234,42 @@ def test_closure_solver_with_zero_network_is_the_plain_solver():
     assert np.abs(sa - sb).max() <= 1e-6 * np.abs(sb).max()
 
 
-def test_closure_solver_step_matches_oracle():
+@pytest.mark.parametrize("every_stage", [True, False])
+def test_closure_solver_step_matches_oracle(every_stage):
     from pyspectral_b200.closure import ClosureSolver
 
     n = 128
     bank = _bank(n, 1, 70)
     net, p = _net_with(n, bank, 5, out_std=0.3)
     net.set_scales(net.inscale, 10.0 * net.outscale)  # a closure term comparable to N
+    gain = np.random.default_rng(5).uniform(0.0, 2.0, net.nshell).astype(np.float32)
+    net.set_shell_gain(gain)
+    kx = np.fft.fftfreq(n, 1.0 / n)[:, None]
+    ky = np.arange(n // 2 + 1)[None, :]
+    g_modes = gain[(np.sqrt(kx ** 2 + ky ** 2) + 0.5).astype(int)]
     cfg = _forced_cfg(n)
-    dev = ClosureSolver(cfg, net)
+    dev = ClosureSolver(cfg, net, every_stage=every_stage)
     st = _random_state(n, 71)
     dev.set_state(st)
 
+    def closure_term(s):
+        fields = co.snapshot_fields(s, 0 * s, 0 * s)[:3].astype(np.float32)
+        S = co.infer_field(p, fields, net.inscale, net.outscale, False)
+        Sh = np.fft.rfft2(S.astype(np.float64)) * dealias_mask(n, 2) * g_modes
+        Sh[0, 0] = 0.0  # the subgrid term carries no mean
+        return Sh
+
     class OracleLES(OracleSolver):
+        held = None
+
         def nonlinear(self, s):
-            fields = co.snapshot_fields(s, 0 * s, 0 * s)[:3].astype(np.float32)
-            S = co.infer_field(p, fields, net.inscale, net.outscale, False)
-            return super().nonlinear(s) + np.fft.rfft2(S.astype(np.float64)) * self.mask
+            S = closure_term(s) if every_stage else self.held
+            return super().nonlinear(s) + S
+
+        def _step(self, dt):
+            # held mode: the network sees the step's initial state only
+            self.held = closure_term(self.state)
+            super()._step(dt)
 
     kw = dict(nu=cfg.nu, alpha=cfg.alpha, alpha_kmax=cfg.alpha_kmax, force_amp=cfg.force_amp,
               force_klo=cfg.force_klo, force_khi=cfg.force_khi)
