@@ -294,6 +294,10 @@ int sp_closure_losses(sp_closure* c, int64_t first, int count, float* host);
  * (row stride row_stride floats), output rows of out_row_stride floats; synchronises. */
 int sp_closure_infer(sp_closure* c, const float* fields, int64_t field_stride, int row_stride,
                      float* out, int out_row_stride, void* stream);
+/* The same launch without the check and the synchronisation (sp_closure_check reports a
+ * timed-out wait later). */
+int sp_closure_infer_async(sp_closure* c, const float* fields, int64_t field_stride,
+                           int row_stride, float* out, int out_row_stride, void* stream);
 /* Attach a closure to a 2D fp32 SP_FFT_CUFFT solver of the same grid before sp_bind: every
  * stage then adds the network's S to the nonlinear term (the sizes sp_query_sizes reports grow
  * to six work fields).  The closure must outlive the solver. */

@@ -94,6 +94,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_closure_step_count": (_i64, [_vp]),
     "sp_closure_losses": (_i, [_vp, _i64, _i, _vp]),
     "sp_closure_infer": (_i, [_vp, _vp, _i64, _i, _vp, _i, _vp]),
+    "sp_closure_infer_async": (_i, [_vp, _vp, _i64, _i, _vp, _i, _vp]),
     "sp_attach_closure": (_i, [_vp, _vp]),
     "sp_closure_check": (_i, [_vp, _vp]),
 }

@@ -220,16 +220,18 @@ class ClosureNet:
         return out
 
     # ------------------------------------------------------------------ inference
-    def infer(self, fields: Any) -> Any:
-        """S at every point from device fields (3, n, n) float32: omega, omega_x, omega_y."""
+    def infer(self, fields: Any, out: Any | None = None, sync: bool = True) -> Any:
+        """S at every point from device fields (3, n, n) float32: omega, omega_x, omega_y.
+        ``sync=False`` only enqueues the launch (``check()`` reports a timed-out wait later)."""
         torch = self.torch
         f = fields.contiguous()
         if tuple(f.shape) != (3, self.n, self.n) or f.dtype != torch.float32 or not f.is_cuda:
             raise ValueError(f"fields must be a float32 CUDA tensor (3, {self.n}, {self.n})")
-        out = torch.empty((self.n, self.n), dtype=torch.float32, device=f.device)
-        self._check(self.lib.sp_closure_infer(self._h, _lib.dptr(f), self.n * self.n, self.n,
-                                              _lib.dptr(out), self.n, self._stream()),
-                    "sp_closure_infer")
+        if out is None:
+            out = torch.empty((self.n, self.n), dtype=torch.float32, device=f.device)
+        fn = self.lib.sp_closure_infer if sync else self.lib.sp_closure_infer_async
+        self._check(fn(self._h, _lib.dptr(f), self.n * self.n, self.n, _lib.dptr(out), self.n,
+                       self._stream()), "sp_closure_infer")
         return out
 
     def check(self) -> None:

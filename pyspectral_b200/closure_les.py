@@ -513,6 +513,33 @@ def run_study(sc: StudyConfig, seed: int = 0, log: Any = None) -> dict[str, Any]
     return out
 
 
+def kernel_demo(n: int = 256, batch_tiles: int = 512, steps: int = 3) -> dict[str, float]:
+    """A few launches of every closure kernel on random data (the small case the kernel
+    profiles are captured on): training steps at a full batch, field inferences, and coarse
+    closure steps in both update modes."""
+    import torch
+
+    rng = np.random.default_rng(0)
+    net = ClosureNet(n, 4)
+    net.load_bank(rng.normal(size=(4, 4, n, n)).astype(np.float32))
+    net.set_params(init_params(0))
+    net.fit_scales()
+    net.set_adam(total_steps=max(steps, 1), warmup=0)
+    losses = net.train(steps, batch_tiles=batch_tiles)
+    f = torch.from_numpy(rng.normal(size=(3, n, n)).astype(np.float32)).to(net.device)
+    for _ in range(steps):
+        net.infer(f)
+    cfg = forced_config(StudyConfig(), n, 5e-6)
+    for every in (False, True):
+        s = ClosureSolver(cfg, net, every_stage=every)
+        s.set_state(random_phase_2d(n, k0=8.0, seed=1, energy=5e-3))
+        for _ in range(steps):
+            s.step(1e-3)
+        s.synchronize()
+    torch.cuda.synchronize()
+    return {"loss_last": float(losses[-1]) if len(losses) else float("nan")}
+
+
 def main(argv: list[str] | None = None) -> int:
     import argparse
     import sys
@@ -522,7 +549,12 @@ def main(argv: list[str] | None = None) -> int:
     ap.add_argument("--out", default=None, help="JSON report path")
     ap.add_argument("--save-net", default=None, help="npz path for the trained network")
     ap.add_argument("--set", nargs="*", default=[], help="StudyConfig overrides key=value")
+    ap.add_argument("--kernels", action="store_true",
+                    help="only launch every closure kernel a few times on random data")
     a = ap.parse_args(argv)
+    if a.kernels:
+        print(json.dumps(kernel_demo()))
+        return 0
     sc = StudyConfig.small() if a.small else StudyConfig()
     for kv in a.set:
         key, val = kv.split("=", 1)

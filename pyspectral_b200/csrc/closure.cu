@@ -1153,8 +1153,8 @@ int sp_closure_losses(sp_closure* c, int64_t first, int count, float* host) {
     return SP_OK;
 }
 
-int sp_closure_infer(sp_closure* c, const float* fields, int64_t field_stride, int row_stride,
-                     float* out, int out_row_stride, void* stream) {
+int sp_closure_infer_async(sp_closure* c, const float* fields, int64_t field_stride,
+                           int row_stride, float* out, int out_row_stride, void* stream) {
     if (!c || !fields || !out || field_stride <= 0 || row_stride < c->n || out_row_stride < c->n)
         return SP_ERR_ARG;
     auto st = (cudaStream_t)stream;
@@ -1164,7 +1164,14 @@ int sp_closure_infer(sp_closure* c, const float* fields, int64_t field_stride, i
         out_row_stride, nullptr, 0, c->err);
     CL_CUDA(cudaGetLastError());
     c->launches += 1;
-    return check_err_flag(c, st, "sp_closure_infer");
+    return SP_OK;
+}
+
+int sp_closure_infer(sp_closure* c, const float* fields, int64_t field_stride, int row_stride,
+                     float* out, int out_row_stride, void* stream) {
+    int r = sp_closure_infer_async(c, fields, field_stride, row_stride, out, out_row_stride, stream);
+    if (r) return r;
+    return check_err_flag(c, (cudaStream_t)stream, "sp_closure_infer");
 }
 
 int sp_filter_spectrum(const void* src, int n_src, void* dst, int n_dst, int dim, int fp64,
