@@ -381,6 +381,9 @@ def ours_ensemble(args, w: dict) -> int:
                    "drag": f"alpha={w['alpha']} on |k|<={w['alpha_kmax']}",
                    "nu": "k_max eta = 1 (nu_for_kmax_eta)", "cfl": w["cfl"],
                    "engine": "sp_batch per size class, one sp_group graph",
+                   "tiles": {str(c.n): c.tile for c in ens.classes},
+                   "tile_source": "TileTuner (CUDA-event timing of each candidate, JSON cache)"
+                   if ens.tuner is not None else "default",
                    "parallelism": "replicas" if world > 1 else "single"},
         "pct_fft_roofline": 100.0 * t_roof / ms_step,
         "fft_roofline": {"t_fft_stage_ms_all_classes": t_fft_stage, "t_roofline_step_ms": t_roof,
@@ -390,6 +393,9 @@ def ours_ensemble(args, w: dict) -> int:
                 "d2h_bytes_per_step": state_bytes / args.steps,
                 "what": "set_states(host) + K steps + get_state of every member, wall clock"},
         "gpu_launches": launches, "clocks": clk,
+        "autotune": None if ens.tuner is None else {
+            k: {"tile": v["tile"], "ms_per_step": v["ms_per_step"], "cached": v["cached"]}
+            for k, v in ens.tuner.report.items()},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = time_oracle_ensemble(w)

@@ -196,6 +196,16 @@ int sp_batch_set_step(sp_batch* b, const double* dt, const double* amp, void* st
 /* Load the states written into u0 (dealias, transpose, stage-0 inputs). */
 int sp_batch_prepare(sp_batch* b, void* stream);
 int sp_batch_step(sp_batch* b, void* stream);
+/* Tile choice of the batched fused passes: sub-blocks per CTA = tile x the default (tile 1;
+ * 2 and 4 are compiled for n <= 1024).  Each sequence is transformed by the same code; the
+ * kernels of different tiles are compiled separately and may contract multiply-adds
+ * differently, so results agree to round-off (bit-identical for a fixed tile; tile 1 is the
+ * single-run engine's).  The ensemble autotuner picks the fastest per size class.
+ * Set it before the first sp_group_step of a group that holds the batch (the group's graph is
+ * captured then); it drops the batch's own step graph. */
+int sp_batch_tile_supported(int n, int tile);
+int sp_batch_set_tile(sp_batch* b, int tile);
+int sp_batch_tile(const sp_batch* b);
 /* Write the members' states back into u0 (NumPy layout) when they changed. */
 int sp_batch_sync_state(sp_batch* b, void* stream);
 /* out[m * 4 + q]: energy, enstrophy, palinstrophy, energy in band_klo <= |k| <= band_khi. */

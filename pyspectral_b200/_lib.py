@@ -63,6 +63,9 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_batch_max_velocity": (_i, [_vp, _dp, _vp]),
     "sp_batch_kernel_launches": (ctypes.c_int64, [_vp]),
     "sp_batch_last_error": (ctypes.c_char_p, [_vp]),
+    "sp_batch_tile_supported": (_i, [_i, _i]),
+    "sp_batch_set_tile": (_i, [_vp, _i]),
+    "sp_batch_tile": (_i, [_vp]),
     "sp_group_create": (_vp, [ctypes.POINTER(_vp), _i, ctypes.POINTER(_i)]),
     "sp_group_destroy": (None, [_vp]),
     "sp_group_step": (_i, [_vp, _vp]),

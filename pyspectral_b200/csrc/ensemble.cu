@@ -30,6 +30,7 @@ size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct sp_batch {
     int n = 0, fp64 = 0, members = 0, nh = 0, kc = 0, nblk = 1;
+    int tile = 1;  // sub-block multiplier of the fused passes (autotuner choice)
     size_t rsize = 4, csize = 8, psize = 16;
     // per-member block of the work buffer: [X | u0t | acct]
     size_t off_u0t = 0, off_acct = 0, member_work = 0;
@@ -104,11 +105,11 @@ int batch_step_kernels(sp_batch* b, cudaStream_t st) {
     void* acct = (char*)b->W + b->off_acct;
     for (int stage = 0; stage < 4; ++stage) {
         B_CUDA(b, sp::fused::row_pass(b->n, b->fp64, X, b->kc, b->base(b->off_tw), st,
-                                      b->members, xs));
+                                      b->members, xs, b->tile));
         B_CUDA(b, sp::fused::col_pass(b->n, b->fp64, stage, X, b->kc, u0t, acct,
                                       b->base(b->off_tab), b->base(b->off_params),
                                       b->base(b->off_tw), st, b->members, xs, us,
-                                      b->tab_stride));
+                                      b->tab_stride, b->tile));
         b->launches += 2;
     }
     return SP_OK;
@@ -258,11 +259,28 @@ int sp_batch_prepare(sp_batch* b, void* stream) {
     B_CUDA(b, sp::fused::transpose_in(b->fp64, b->u0, u0t, b->n, b->kc, st, b->members, u0s, us));
     B_CUDA(b, sp::fused::col_pass(b->n, b->fp64, -1, b->W, b->kc, u0t, (char*)b->W + b->off_acct,
                                   b->base(b->off_tab), b->base(b->off_params), b->base(b->off_tw),
-                                  st, b->members, b->member_work / b->psize, us, b->tab_stride));
+                                  st, b->members, b->member_work / b->psize, us, b->tab_stride,
+                                  b->tile));
     b->launches += 3;
     b->fresh = true;
     return SP_OK;
 }
+
+int sp_batch_tile_supported(int n, int tile) { return sp::fused::tile_supported(n, tile) ? 1 : 0; }
+
+int sp_batch_set_tile(sp_batch* b, int tile) {
+    if (!b) return SP_ERR_ARG;
+    if (!sp::fused::tile_supported(b->n, tile))
+        return bfail(b, SP_ERR_ARG, "sp_batch_set_tile", "tile not compiled for this grid");
+    if (tile != b->tile && b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    b->tile = tile;
+    return SP_OK;
+}
+
+int sp_batch_tile(const sp_batch* b) { return b ? b->tile : -1; }
 
 int sp_batch_step(sp_batch* b, void* stream) {
     if (!b) return SP_ERR_ARG;

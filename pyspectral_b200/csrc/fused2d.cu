@@ -9,41 +9,73 @@ namespace fused {
 
 namespace {
 
-template <typename T, int N>
-cudaError_t attrs() {
-    using F = Fused2D<N>;
-    const int row_smem = (int)RowSingle<N>::smem_bytes(sizeof(cplx<T>));
-    const int max_smem = (int)RowPairs<N>::smem_bytes(sizeof(Pair<T>));
-    const int col_smem = (int)F::template smem_bytes<Pair<T>>();
-    cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_row_pass<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  row_smem)))
-        return e;
-    if ((e = cudaFuncSetAttribute(k_row_max<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  max_smem)))
-        return e;
-    if ((e = cudaFuncSetAttribute(k_col_pass<T, N, -1>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
-        return e;
-    if ((e = cudaFuncSetAttribute(k_col_pass<T, N, 0>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
-        return e;
-    if ((e = cudaFuncSetAttribute(k_col_pass<T, N, 1>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
-        return e;
-    if ((e = cudaFuncSetAttribute(k_col_pass<T, N, 2>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
-        return e;
-    return cudaFuncSetAttribute(k_col_pass<T, N, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                col_smem);
+// Tile multipliers compiled for a grid: 1, 2, 4 up to n = 1024 (CTAs of at most 256 threads),
+// 1 above.
+constexpr bool tile_ok(int n, int bx) { return bx == 1 || ((bx == 2 || bx == 4) && n <= 1024); }
+
+template <typename T, int N, int BX>
+cudaError_t attrs_tile() {
+    if constexpr (!tile_ok(N, BX)) {
+        return cudaSuccess;
+    } else {
+        using F = Fused2D<N, BX>;
+        const int row_smem = (int)RowSingle<N, BX>::smem_bytes(sizeof(cplx<T>));
+        const int col_smem = (int)F::template smem_bytes<Pair<T>>();
+        cudaError_t e;
+        if ((e = cudaFuncSetAttribute(k_row_pass<T, N, BX>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, row_smem)))
+            return e;
+        if ((e = cudaFuncSetAttribute(k_col_pass<T, N, -1, BX>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
+            return e;
+        if ((e = cudaFuncSetAttribute(k_col_pass<T, N, 0, BX>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
+            return e;
+        if ((e = cudaFuncSetAttribute(k_col_pass<T, N, 1, BX>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
+            return e;
+        if ((e = cudaFuncSetAttribute(k_col_pass<T, N, 2, BX>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem)))
+            return e;
+        return cudaFuncSetAttribute(k_col_pass<T, N, 3, BX>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem);
+    }
 }
 
 template <typename T, int N>
-cudaError_t row(void* X, int kc, const void* tw, cudaStream_t st, int members, size_t xs) {
-    using F = RowSingle<N>;
-    k_row_pass<T, N><<<dim3(N / F::B, members), F::THREADS, F::smem_bytes(sizeof(cplx<T>)), st>>>(
-        (Pair<T>*)X, kc, (const cplx<T>*)tw, xs);
-    return cudaGetLastError();
+cudaError_t attrs() {
+    const int max_smem = (int)RowPairs<N>::smem_bytes(sizeof(Pair<T>));
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_row_max<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  max_smem)))
+        return e;
+    if ((e = attrs_tile<T, N, 1>())) return e;
+    if ((e = attrs_tile<T, N, 2>())) return e;
+    return attrs_tile<T, N, 4>();
+}
+
+template <typename T, int N, int BX>
+cudaError_t row_tile(void* X, int kc, const void* tw, cudaStream_t st, int members, size_t xs) {
+    if constexpr (!tile_ok(N, BX)) {
+        return cudaErrorInvalidValue;
+    } else {
+        using F = RowSingle<N, BX>;
+        k_row_pass<T, N, BX><<<dim3(N / F::B, members), F::THREADS,
+                               F::smem_bytes(sizeof(cplx<T>)), st>>>((Pair<T>*)X, kc,
+                                                                     (const cplx<T>*)tw, xs);
+        return cudaGetLastError();
+    }
+}
+
+template <typename T, int N>
+cudaError_t row(void* X, int kc, const void* tw, cudaStream_t st, int members, size_t xs,
+                int tile) {
+    switch (tile) {
+        case 1: return row_tile<T, N, 1>(X, kc, tw, st, members, xs);
+        case 2: return row_tile<T, N, 2>(X, kc, tw, st, members, xs);
+        case 4: return row_tile<T, N, 4>(X, kc, tw, st, members, xs);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 template <typename T, int N>
@@ -68,27 +100,42 @@ struct ColArgs {
     int members;
     size_t xs, us;
     int ts;
+    int tile;
 };
 
-template <typename T, int N, int STAGE>
+template <typename T, int N, int STAGE, int BX>
 cudaError_t col_stage(const ColArgs& a) {
-    using F = Fused2D<N>;
-    const int grid = (a.kc + F::B - 1) / F::B;
-    k_col_pass<T, N, STAGE><<<dim3(grid, a.members), F::THREADS,
-                              F::template smem_bytes<Pair<T>>(), a.st>>>(
-        (Pair<T>*)a.X, a.kc, (cplx<T>*)a.u0t, (cplx<T>*)a.acct, (const T*)a.tab,
-        (const StepParams<T>*)a.P, (const cplx<T>*)a.tw, a.xs, a.us, a.ts);
-    return cudaGetLastError();
+    if constexpr (!tile_ok(N, BX)) {
+        return cudaErrorInvalidValue;
+    } else {
+        using F = Fused2D<N, BX>;
+        const int grid = (a.kc + F::B - 1) / F::B;
+        k_col_pass<T, N, STAGE, BX><<<dim3(grid, a.members), F::THREADS,
+                                      F::template smem_bytes<Pair<T>>(), a.st>>>(
+            (Pair<T>*)a.X, a.kc, (cplx<T>*)a.u0t, (cplx<T>*)a.acct, (const T*)a.tab,
+            (const StepParams<T>*)a.P, (const cplx<T>*)a.tw, a.xs, a.us, a.ts);
+        return cudaGetLastError();
+    }
+}
+
+template <typename T, int N, int BX>
+cudaError_t col_tile(int stage, const ColArgs& a) {
+    switch (stage) {
+        case -1: return col_stage<T, N, -1, BX>(a);
+        case 0: return col_stage<T, N, 0, BX>(a);
+        case 1: return col_stage<T, N, 1, BX>(a);
+        case 2: return col_stage<T, N, 2, BX>(a);
+        case 3: return col_stage<T, N, 3, BX>(a);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 template <typename T, int N>
 cudaError_t col(int stage, const ColArgs& a) {
-    switch (stage) {
-        case -1: return col_stage<T, N, -1>(a);
-        case 0: return col_stage<T, N, 0>(a);
-        case 1: return col_stage<T, N, 1>(a);
-        case 2: return col_stage<T, N, 2>(a);
-        case 3: return col_stage<T, N, 3>(a);
+    switch (a.tile) {
+        case 1: return col_tile<T, N, 1>(stage, a);
+        case 2: return col_tile<T, N, 2>(stage, a);
+        case 4: return col_tile<T, N, 4>(stage, a);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -174,6 +221,8 @@ void fill_twiddles(int n, double* out) {
     });
 }
 
+bool tile_supported(int n, int tile) { return tile_ok(n, tile); }
+
 bool supported(int n, int fp64) {
     if (n < 16 || (n & (n - 1))) return false;
     return fp64 ? n <= 4096 : n <= 8192;
@@ -184,9 +233,9 @@ cudaError_t set_attributes(int n, int fp64) {
 }
 
 cudaError_t row_pass(int n, int fp64, void* X, int kc, const void* tw, cudaStream_t st,
-                     int members, size_t x_stride) {
+                     int members, size_t x_stride, int tile) {
     return dispatch(n, fp64, [&]<typename T, int N>() {
-        return row<T, N>(X, kc, tw, st, members, x_stride);
+        return row<T, N>(X, kc, tw, st, members, x_stride, tile);
     });
 }
 
@@ -199,8 +248,8 @@ cudaError_t row_max(int n, int fp64, const void* X, int kc, const void* tw,
 
 cudaError_t col_pass(int n, int fp64, int stage, void* X, int kc, void* u0t, void* acct,
                      const void* tab, const void* params, const void* tw, cudaStream_t st,
-                     int members, size_t x_stride, size_t u_stride, int tab_stride) {
-    ColArgs a{X, kc, u0t, acct, tab, params, tw, st, members, x_stride, u_stride, tab_stride};
+                     int members, size_t x_stride, size_t u_stride, int tab_stride, int tile) {
+    ColArgs a{X, kc, u0t, acct, tab, params, tw, st, members, x_stride, u_stride, tab_stride, tile};
     return dispatch(n, fp64, [&]<typename T, int N>() { return col<T, N>(stage, a); });
 }
 

@@ -35,10 +35,17 @@ constexpr int sub_blocks(int t, int count) {
     return b < count ? b : count;
 }
 
-template <int N>
+// BX: tile multiplier chosen by the ensemble autotuner (1, 2 or 4 times the default sub-blocks
+// per CTA; the single-run engine uses 1).
+constexpr int tiled_blocks(int t, int count, int bx) {
+    const int b = sub_blocks(t, count) * bx;
+    return b < count ? b : count;
+}
+
+template <int N, int BX = 1>
 struct Fused2D {
     static constexpr int T = N / 16;
-    static constexpr int B = sub_blocks(T, N);
+    static constexpr int B = tiled_blocks(T, N, BX);
     static constexpr int THREADS = T * B;
     template <typename E>
     static constexpr size_t smem_bytes() { return (size_t)B * FftPlan<N>::SMEM * sizeof(E); }
@@ -77,22 +84,20 @@ struct RowPairs {
 
 // Rows per CTA for the row pass: single-row sub-blocks (see sub_blocks), two CTAs resident
 // per SM at n = 8192 (64 registers per thread at 512 threads).
-template <int N>
+template <int N, int BX = 1>
 struct RowSingle {
     static constexpr int T = N / 16;
-    static constexpr int B = sub_blocks(T, N);
+    static constexpr int B = tiled_blocks(T, N, BX);
     static constexpr int THREADS = T * B;
     static constexpr size_t smem_bytes(size_t elem) { return (size_t)B * FftPlan<N>::SMEM * elem; }
 };
 
 // Batched launches: blockIdx.y selects the member; each member's arrays start `stride`
 // elements after the previous member's (stride 0 for a single run).
-template <typename T, int N>
-__global__ void __launch_bounds__(RowSingle<N>::THREADS, 2) k_row_pass(Pair<T>* __restrict__ X,
-                                                                      int kc,
-                                                                      const cplx<T>* __restrict__ tw,
-                                                                      size_t x_stride) {
-    using F = RowSingle<N>;
+template <typename T, int N, int BX = 1>
+__global__ void __launch_bounds__(RowSingle<N, BX>::THREADS, 2) k_row_pass(
+    Pair<T>* __restrict__ X, int kc, const cplx<T>* __restrict__ tw, size_t x_stride) {
+    using F = RowSingle<N, BX>;
     constexpr int TT = F::T;
     constexpr int RI = first_radix<N, true>();   // inverse input pattern
     constexpr int RF = last_radix<N, false>();   // forward output pattern
@@ -206,12 +211,12 @@ __device__ __forceinline__ Pair<T> next_inputs(T kx, T ky, T k2, bool keep, cplx
 
 // STAGE 0..3: Lawson stage; STAGE = -1: set-up (no forward transform, no update: the inputs of
 // stage 0 from the state u0t).
-template <typename T, int N, int STAGE>
-__global__ void __launch_bounds__(Fused2D<N>::THREADS) k_col_pass(
+template <typename T, int N, int STAGE, int BX = 1>
+__global__ void __launch_bounds__(Fused2D<N, BX>::THREADS) k_col_pass(
     Pair<T>* __restrict__ X, int kc, cplx<T>* __restrict__ u0t, cplx<T>* __restrict__ acct,
     const T* __restrict__ tab, const StepParams<T>* __restrict__ P,
     const cplx<T>* __restrict__ tw, size_t x_stride, size_t u_stride, int tab_stride) {
-    using F = Fused2D<N>;
+    using F = Fused2D<N, BX>;
     constexpr int TT = F::T;
     constexpr int RF0 = first_radix<N, false>();  // forward input pattern
     constexpr int RL = last_radix<N, false>();    // forward output = inverse input pattern

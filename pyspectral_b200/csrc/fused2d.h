@@ -21,8 +21,11 @@ void fill_twiddles(int n, double* out);
 
 // Batched forms: `members` independent runs of the same grid, member m's arrays `*_stride`
 // elements after member m-1's (X in Pair units, u0/u0t/acct in complex units, tab in reals).
+// tile: sub-block multiplier of the row and column passes (1; 2 and 4 for n <= 1024), the
+// ensemble autotuner's choice.
+bool tile_supported(int n, int tile);
 cudaError_t row_pass(int n, int fp64, void* X, int kc, const void* tw, cudaStream_t st,
-                     int members = 1, size_t x_stride = 0);
+                     int members = 1, size_t x_stride = 0, int tile = 1);
 cudaError_t row_max(int n, int fp64, const void* X, int kc, const void* tw,
                     unsigned long long* umax, cudaStream_t st, int members = 1,
                     size_t x_stride = 0);
@@ -31,7 +34,7 @@ cudaError_t row_max(int n, int fp64, const void* X, int kc, const void* tw,
 cudaError_t col_pass(int n, int fp64, int stage, void* X, int kc, void* u0t, void* acct,
                      const void* tab, const void* params, const void* tw, cudaStream_t st,
                      int members = 1, size_t x_stride = 0, size_t u_stride = 0,
-                     int tab_stride = 0);
+                     int tab_stride = 0, int tile = 1);
 cudaError_t transpose_in(int fp64, const void* u0, void* u0t, int n, int kc, cudaStream_t st,
                          int members = 1, size_t u0_stride = 0, size_t u_stride = 0);
 cudaError_t transpose_out(int fp64, const void* u0t, void* u0, int n, int kc, cudaStream_t st,

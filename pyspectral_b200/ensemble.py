@@ -14,9 +14,12 @@ with the same configuration and the same dt / amplitude sequence computes (bit f
 from __future__ import annotations
 
 import ctypes
+import json
 import math
+import os
 import weakref
 from collections.abc import Sequence
+from pathlib import Path
 from typing import Any
 
 import numpy as np
@@ -37,6 +40,84 @@ def nu_for_kmax_eta(n: int, power: float, k_force: float, kmax_eta: float = 1.0)
     """
     beta = k_force * k_force * power
     return beta ** (1.0 / 3.0) * (kmax_eta / (n / 3.0)) ** 2
+
+
+TILES = (1, 2, 4)
+
+
+def tune_cache_path() -> Path:
+    """JSON cache of tile choices (PYSPECTRAL_B200_TUNE_CACHE, else ~/.cache/pyspectral_b200)."""
+    p = os.environ.get("PYSPECTRAL_B200_TUNE_CACHE")
+    return Path(p) if p else Path.home() / ".cache" / "pyspectral_b200" / "tiles.json"
+
+
+def load_tune_cache(path: Path) -> dict[str, Any]:
+    try:
+        data = json.loads(Path(path).read_text())
+        return data if isinstance(data, dict) else {}
+    except (OSError, ValueError):
+        return {}
+
+
+def save_tune_cache(path: Path, data: dict[str, Any]) -> None:
+    path = Path(path)
+    try:
+        path.parent.mkdir(parents=True, exist_ok=True)
+        tmp = path.with_suffix(".tmp")
+        tmp.write_text(json.dumps(data, indent=1, sort_keys=True))
+        tmp.replace(path)
+    except OSError:
+        pass  # a read-only home only loses the cache
+
+
+def tune_key(gpu: str, n: int, fp64: bool, members: int) -> str:
+    return f"{gpu}|n={n}|{'fp64' if fp64 else 'fp32'}|members={members}"
+
+
+class TileTuner:
+    """Chooses each size class's tile (sub-blocks per CTA of the fused row and column passes,
+    1, 2 or 4 times the default) by timing the class's batched step on the device (CUDA
+    events, ``reps`` steps after two warm-up steps); choices are cached in a JSON file keyed by
+    GPU model, grid, precision and member count.  Tiles change results at round-off only."""
+
+    def __init__(self, path: Path | None = None, reps: int = 5) -> None:
+        self.path = Path(path) if path is not None else tune_cache_path()
+        self.reps = reps
+        self.cache = load_tune_cache(self.path)
+        self.report: dict[str, Any] = {}
+
+    def choose(self, sc: _SizeClass, stream: Any) -> int:
+        torch, lib = sc.torch, sc.lib
+        gpu = torch.cuda.get_device_name(sc.u0.device)
+        key = tune_key(gpu, sc.n, sc.fp64, sc.count)
+        cands = [t for t in TILES if lib.sp_batch_tile_supported(sc.n, t)]
+        hit = self.cache.get(key)
+        if isinstance(hit, dict) and hit.get("tile") in cands:
+            self.report[key] = dict(hit, cached=True)
+            return int(hit["tile"])
+        if len(cands) == 1:
+            return cands[0]
+        sc.set_step(np.full(sc.count, 1e-4), np.zeros(sc.count), stream)
+        sc._check(lib.sp_batch_prepare(sc.h, stream), "sp_batch_prepare")
+        times: dict[int, float] = {}
+        cur = torch.cuda.current_stream(sc.u0.device)
+        for t in cands:
+            sc._check(lib.sp_batch_set_tile(sc.h, t), "sp_batch_set_tile")
+            for _ in range(2):
+                sc._check(lib.sp_batch_step(sc.h, stream), "sp_batch_step")
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(cur)
+            for _ in range(self.reps):
+                sc._check(lib.sp_batch_step(sc.h, stream), "sp_batch_step")
+            e1.record(cur)
+            e1.synchronize()
+            times[t] = e0.elapsed_time(e1) / self.reps
+        best = min(times, key=times.get)
+        entry = {"tile": best, "ms_per_step": {str(k): v for k, v in times.items()}}
+        self.cache[key] = entry
+        self.report[key] = dict(entry, cached=False)
+        save_tune_cache(self.path, self.cache)
+        return best
 
 
 class _SizeClass:
@@ -83,6 +164,13 @@ class _SizeClass:
             raise _lib.EngineError(f"{what} failed ({_lib.STATUS_NAMES.get(status)}): "
                                    f"{msg.decode()}")
 
+    def set_tile(self, tile: int) -> None:
+        self._check(self.lib.sp_batch_set_tile(self.h, int(tile)), "sp_batch_set_tile")
+
+    @property
+    def tile(self) -> int:
+        return int(self.lib.sp_batch_tile(self.h))
+
     def set_step(self, dt: np.ndarray, amp: np.ndarray, stream: Any) -> None:
         dt = np.ascontiguousarray(dt, dtype=np.float64)
         amp = np.ascontiguousarray(amp, dtype=np.float64)
@@ -97,10 +185,11 @@ class Ensemble:
 
     ``members``: one :class:`Config` per run (dim 2; n a power of two, 16..8192 fp32 /
     16..4096 fp64).  Runs of the same n and dtype form a size class and must share drag and
-    forcing band; viscosity, time step and forcing amplitude are per run.
+    forcing band; viscosity, time step and forcing amplitude are per run.  ``autotune``: pick
+    each class's tile with :class:`TileTuner` (default on, see PYSPECTRAL_B200_AUTOTUNE).
     """
 
-    def __init__(self, members: Sequence[Config]) -> None:
+    def __init__(self, members: Sequence[Config], autotune: bool | None = None) -> None:
         import torch
 
         from pyspectral_b200.solver import _cuda_reason
@@ -126,6 +215,16 @@ class Ensemble:
                 self.where[i] = (ci, slot)
         self.index = [[i for i in range(len(self.members)) if self.where[i][0] == ci]
                       for ci in range(len(self.classes))]
+        # tile choices: the autotuner (default; PYSPECTRAL_B200_AUTOTUNE=0 keeps tile 1), before
+        # the group graph is captured
+        if autotune is None:
+            autotune = os.environ.get("PYSPECTRAL_B200_AUTOTUNE", "1") != "0"
+        self.tuner: TileTuner | None = None
+        if autotune:
+            self.tuner = TileTuner()
+            st = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+            for c in self.classes:
+                c.set_tile(self.tuner.choose(c, st))
         arr = (ctypes.c_void_p * len(self.classes))(*[c.h for c in self.classes])
         st = ctypes.c_int(0)
         g = lib.sp_group_create(arr, len(self.classes), ctypes.byref(st))
@@ -259,6 +358,11 @@ class Ensemble:
                 "sp_batch_diagnostics")
             out[self.index[ci]] = buf[:, 3]
         return out
+
+    @property
+    def tiles(self) -> list[int]:
+        """Tile of each size class (sorted by n, dtype)."""
+        return [c.tile for c in self.classes]
 
     @property
     def kernel_launches(self) -> int:

@@ -34,7 +34,7 @@ def test_members_equal_single_runs_bit_for_bit(dtype):
 
     cfgs = _members(dtype)
     ics = _ics(cfgs)
-    ens = Ensemble(cfgs)
+    ens = Ensemble(cfgs, autotune=False)  # tile 1: the single-run engine's kernels
     ens.set_states(ics)
     dts = [np.array([1e-3 * (1 + 0.1 * i + 0.05 * k) for i in range(len(cfgs))]) for k in range(6)]
     amps = [np.array([0.2 + 0.02 * i + 0.01 * k for i in range(len(cfgs))]) for k in range(6)]
@@ -137,3 +137,53 @@ def test_ensemble_rejects_unsupported_members():
         Ensemble([Config(n=32, dim=2, alpha=0.1), Config(n=32, dim=2, alpha=0.2)])
     assert math.isclose(__import__("pyspectral_b200.ensemble", fromlist=["x"]).nu_for_kmax_eta(
         384, 1e-3, 11.0), (121e-3) ** (1 / 3) * (1 / 128) ** 2)
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_every_tile_gives_the_same_members(dtype):
+    """The autotuner's choice (sub-blocks per CTA of the fused passes) leaves the arithmetic of
+    every sequence alone; separately compiled kernels may contract multiply-adds differently, so
+    tiles agree to round-off (bit-identical runs need a fixed tile)."""
+    from pyspectral_b200.ensemble import Ensemble
+
+    cfgs = [Config(n=n, dim=2, nu=2e-3, alpha=0.1, alpha_kmax=2.0, force_amp=0.2, force_klo=3,
+                   force_khi=5, dtype=dtype) for n in (16, 64, 256, 1024) for _ in range(2)]
+    ics = [initial.random_phase_2d(c.n, k0=c.n / 10, seed=3 + i) for i, c in enumerate(cfgs)]
+    out = {}
+    for tile in (1, 2, 4):
+        ens = Ensemble(cfgs, autotune=False)
+        for c in ens.classes:
+            c.set_tile(tile)
+        assert ens.tiles == [tile] * len(ens.classes)
+        ens.set_states(ics)
+        for k in range(3):
+            ens.step(1e-3 * (1 + 0.1 * k))
+        out[tile] = [ens.get_state(i) for i in range(len(cfgs))]
+    tol = 1e-13 if dtype == "float64" else 2e-6
+    for tile in (2, 4):
+        for i in range(len(cfgs)):
+            ref = out[1][i]
+            assert np.abs(out[tile][i] - ref).max() <= tol * np.abs(ref).max(), (tile, i)
+
+
+def test_autotuner_times_candidates_and_caches(tmp_path, monkeypatch):
+    import json
+
+    from pyspectral_b200.ensemble import Ensemble, tune_key
+
+    monkeypatch.setenv("PYSPECTRAL_B200_TUNE_CACHE", str(tmp_path / "tiles.json"))
+    cfgs = [Config(n=n, dim=2, nu=2e-3, dtype="float32") for n in (128, 128, 256, 2048)]
+    ens = Ensemble(cfgs, autotune=True)
+    rep = ens.tuner.report
+    data = json.loads((tmp_path / "tiles.json").read_text())
+    import torch
+
+    gpu = torch.cuda.get_device_name(0)
+    for n, m in ((128, 2), (256, 1)):
+        e = data[tune_key(gpu, n, False, m)]
+        assert set(e["ms_per_step"]) == {"1", "2", "4"} and e["tile"] in (1, 2, 4)
+        assert rep[tune_key(gpu, n, False, m)]["cached"] is False
+    assert ens.tiles[-1] == 1  # 2048^2: only tile 1 is compiled
+    again = Ensemble(cfgs, autotune=True)
+    assert again.tuner.report[tune_key(gpu, 128, False, 2)]["cached"] is True
+    assert again.tiles == ens.tiles

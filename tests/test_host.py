@@ -291,3 +291,16 @@ def test_cli_list_reports_every_variant(capsys):
     assert main(["list"]) == 0
     out = capsys.readouterr().out
     assert "b200/fused-fft-graph" in out and "b200/fused-inplace-graph" in out
+
+
+def test_tile_tuner_cache_roundtrip(tmp_path):
+    from pyspectral_b200.ensemble import load_tune_cache, save_tune_cache, tune_key
+
+    p = tmp_path / "sub" / "tiles.json"
+    assert load_tune_cache(p) == {}
+    k = tune_key("NVIDIA B200", 512, True, 64)
+    assert k == "NVIDIA B200|n=512|fp64|members=64"
+    save_tune_cache(p, {k: {"tile": 2, "ms_per_step": {"1": 1.0, "2": 0.8}}})
+    assert load_tune_cache(p)[k]["tile"] == 2
+    p.write_text("not json")
+    assert load_tune_cache(p) == {}
