@@ -297,16 +297,20 @@ def time_oracle_ensemble(w: dict) -> dict:
     return {"sec_per_step": total_s, "mpts": pts / total_s / 1e6, "cores": os.cpu_count() or 1}
 
 
-def ensemble_fft_stage_ms(w: dict) -> float:
+def ensemble_fft_stage_ms(w: dict, counts: dict | None = None) -> float:
     """Standalone batched cuFFT time of one RK stage for every class (2 C2R + 2 R2C per member,
-    batched over the class, through torch.fft), summed over the classes."""
+    batched over the class, through torch.fft), summed over the classes; ``counts`` = members
+    per size (default: the workload's)."""
     import torch
 
     cdt = torch.complex64 if w["dtype"] == "float32" else torch.complex128
     rdt = torch.float32 if w["dtype"] == "float32" else torch.float64
     tot = 0.0
     for n in w["sizes"]:
-        b = 2 * w["per_size"]
+        m = w["per_size"] if counts is None else counts.get(n, 0)
+        if m == 0:
+            continue
+        b = 2 * m
         q = torch.zeros((b, n, n // 2 + 1), dtype=cdt, device="cuda")
         r = torch.zeros((b, n, n), dtype=rdt, device="cuda")
 
@@ -323,57 +327,66 @@ def ensemble_fft_stage_ms(w: dict) -> float:
 
 
 def ours_ensemble(args, w: dict) -> int:
+    """The ensemble workload.  Under torchrun the members are partitioned over the ranks by
+    balanced grid points (sharding.partition_by_points) and each GPU advances its share: the
+    value is all members' points over the slowest rank's step time (scaling "strong")."""
     import torch
 
-    from pyspectral_b200.ensemble import Ensemble
+    from pyspectral_b200.sharding import Comm, ShardedEnsemble
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    comm = Replicas("nccl", torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    comm = Replicas("nccl", dev)
     members = ensemble_members(w)
     ics = ensemble_ics(w, members)
-    ens = Ensemble(members)
-    ens.set_states(ics)
-    ens.run_steps(args.warmup, cfl=w["cfl"], target_power=w["power"])
+    se = ShardedEnsemble(members, comm=Comm(dev))
+    ens = se.ens
+    counts = {n: sum(1 for i in se.local if members[i].n == n) for n in w["sizes"]}
+    se.set_states(ics)
+    se.run_steps(args.warmup, cfl=w["cfl"], target_power=w["power"])
     torch.cuda.synchronize()
     comm.barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    l0 = ens.kernel_launches
+    l0 = ens.kernel_launches if ens is not None else 0
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
-    ens.run_steps(args.steps, cfl=w["cfl"], target_power=w["power"])
+    se.run_steps(args.steps, cfl=w["cfl"], target_power=w["power"])
     ev1.record()
     ev1.synchronize()
     comm.barrier()
     clk = clocks.stop()
-    launches = ens.kernel_launches - l0
+    launches = (ens.kernel_launches - l0) if ens is not None else 0
     ms_step = comm.max(ev0.elapsed_time(ev1)) / args.steps
     pts = sum(float(c.n) ** 2 for c in members)
-    value = aggregate_mpts(world, pts, ms_step * 1e-3)
-    # end to end: host states in, K steps, host states out
-    e2 = Ensemble(members)
+    value = pts / (ms_step * 1e-3) / 1e6
+    # end to end: host states in, K steps, host states out (this rank's members)
+    e2 = ShardedEnsemble(members, comm=Comm(dev))
     e2.set_states(ics)
     torch.cuda.synchronize()
     comm.barrier()
     t0 = time.perf_counter()
     e2.set_states(ics)
     e2.run_steps(args.steps, cfl=w["cfl"], target_power=w["power"])
-    outs = [e2.get_state(i) for i in range(len(members))]
+    outs = [e2.ens.get_state(i) for i in range(len(e2.local))] if e2.ens is not None else []
     e2e_s = comm.max(time.perf_counter() - t0)
-    state_bytes = sum(c.u0.nbytes for c in e2.classes)
+    state_bytes = sum(c.u0.nbytes for c in e2.ens.classes) if e2.ens is not None else 0
+    state_bytes = int(comm.max(float(state_bytes)) * world)
     del e2, outs
     torch.cuda.empty_cache()
-    # aggregate FFT roofline of the reference's definition, summed over the classes
-    t_fft_stage = ensemble_fft_stage_ms(w)
+    # FFT roofline of the reference's definition for this rank's members; the job's is the
+    # slowest rank's
+    t_fft_stage = ensemble_fft_stage_ms(w, counts)
     bcopy = copy_bandwidth_gbs()
-    pw = sum(w["per_size"] * traffic_model(n, 2, "basdevant", w["dtype"])["pointwise_bytes"]
+    pw = sum(counts[n] * traffic_model(n, 2, "basdevant", w["dtype"])["pointwise_bytes"]
              for n in w["sizes"])
-    t_roof = 4 * t_fft_stage + pw / (bcopy * 1e9) * 1e3
+    t_roof = comm.max(4 * t_fft_stage + pw / (bcopy * 1e9) * 1e3)
     line = {
         "metric": "Mpts/s/RK4 step", "value": value, "unit": "Mpts/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
+        "vs_baseline": None,
         "dtype": "f32" if w["dtype"] == "float32" else "f64", "data": "synthetic",
         "config": {"workload": args.workload, "sizes": list(w["sizes"]),
                    "runs_per_size": w["per_size"], "members": len(members),
@@ -381,19 +394,20 @@ def ours_ensemble(args, w: dict) -> int:
                    "drag": f"alpha={w['alpha']} on |k|<={w['alpha_kmax']}",
                    "nu": "k_max eta = 1 (nu_for_kmax_eta)", "cfl": w["cfl"],
                    "engine": "sp_batch per size class, one sp_group graph",
-                   "tiles": {str(c.n): c.tile for c in ens.classes},
+                   "tiles": {str(c.n): c.tile for c in ens.classes} if ens is not None else {},
                    "tile_source": "TileTuner (CUDA-event timing of each candidate, JSON cache)"
-                   if ens.tuner is not None else "default",
-                   "parallelism": "replicas" if world > 1 else "single"},
+                   if ens is not None and ens.tuner is not None else "default",
+                   "parallelism": (f"members partitioned over {world} ranks by grid points"
+                                   if world > 1 else "single")},
         "pct_fft_roofline": 100.0 * t_roof / ms_step,
-        "fft_roofline": {"t_fft_stage_ms_all_classes": t_fft_stage, "t_roofline_step_ms": t_roof,
-                         "copy_bw_gbs": bcopy, "pointwise_bytes": pw},
-        "e2e": {"value": aggregate_mpts(world, pts * args.steps, e2e_s), "unit": "Mpts/s",
+        "fft_roofline": {"t_roofline_step_ms": t_roof, "copy_bw_gbs": bcopy,
+                         "t_fft_stage_ms_local_classes": t_fft_stage, "pointwise_bytes_local": pw},
+        "e2e": {"value": pts * args.steps / e2e_s / 1e6, "unit": "Mpts/s",
                 "h2d_bytes_per_step": state_bytes / args.steps,
                 "d2h_bytes_per_step": state_bytes / args.steps,
                 "what": "set_states(host) + K steps + get_state of every member, wall clock"},
         "gpu_launches": launches, "clocks": clk,
-        "autotune": None if ens.tuner is None else {
+        "autotune": None if ens is None or ens.tuner is None else {
             k: {"tile": v["tile"], "ms_per_step": v["ms_per_step"], "cached": v["cached"]}
             for k, v in ens.tuner.report.items()},
     }

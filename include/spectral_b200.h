@@ -298,6 +298,14 @@ int sp_closure_grad(sp_closure* c, int64_t step, int batch_tiles, uint64_t seed,
 /* `steps` Adam steps at batch_tiles tiles each (graph-replayed in chunks); synchronises. */
 int sp_closure_train(sp_closure* c, int steps, int batch_tiles, uint64_t seed, void* stream);
 int64_t sp_closure_step_count(const sp_closure* c);
+/* One optimiser step split around a gradient exchange (data-parallel training over ranks):
+ * _begin runs the forward/backward kernels and leaves this rank's batch gradient (15440 fp32)
+ * in the device buffer sp_closure_grad_buffer returns; the caller may replace it there (e.g.
+ * by the mean over ranks with an NCCL all-reduce on the same stream); _finish applies Adam.
+ * Nothing synchronises; sp_closure_check reports a timed-out wait. */
+int sp_closure_train_begin(sp_closure* c, int batch_tiles, uint64_t seed, void* stream);
+int sp_closure_train_finish(sp_closure* c, void* stream);
+void* sp_closure_grad_buffer(sp_closure* c);
 /* Mean loss of steps first .. first+count-1 (the last 65536 steps are kept). */
 int sp_closure_losses(sp_closure* c, int64_t first, int count, float* host);
 /* S at every point of an n x n field: inputs omega, omega_x, omega_y at fields + f*field_stride

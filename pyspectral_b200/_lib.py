@@ -95,6 +95,9 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_closure_grad": (_i, [_vp, _i64, _i, _u64, _vp]),
     "sp_closure_train": (_i, [_vp, _i, _i, _u64, _vp]),
     "sp_closure_step_count": (_i64, [_vp]),
+    "sp_closure_train_begin": (_i, [_vp, _i, _u64, _vp]),
+    "sp_closure_train_finish": (_i, [_vp, _vp]),
+    "sp_closure_grad_buffer": (_vp, [_vp]),
     "sp_closure_losses": (_i, [_vp, _i64, _i, _vp]),
     "sp_closure_infer": (_i, [_vp, _vp, _i64, _i, _vp, _i, _vp]),
     "sp_closure_infer_async": (_i, [_vp, _vp, _i64, _i, _vp, _i, _vp]),

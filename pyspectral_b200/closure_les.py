@@ -67,7 +67,7 @@ class StudyConfig:
     t_settle: float = 5.0
     train_seeds: int = 16
     snapshots: int = 4000
-    snap_every: int = 100
+    snap_every: int = 250
     test_seeds: int = 16
     test_seed0: int = 1000
     val_seeds: int = 4

@@ -282,10 +282,12 @@ struct TrainSmem {
     static constexpr int DZ = H2 + kTile * kK * 2;               // [128 x 64]
     static constexpr int ST = DZ + kTile * kH * 2;               // stencil floats
     static constexpr int W4 = ST + kStencil * 4;                 // w4 fp32 [80]
-    static constexpr int DW4 = W4 + kK * 4;                      // dw4 partial fp32 [80]
-    static constexpr int BYTES = DW4 + kK * 4;
+    static constexpr int DW4 = W4 + kK * 4;                      // dw4 partials fp32 [4][80]
+    static constexpr int BYTES = DW4 + 4 * kK * 4;
 };
 static_assert(TrainSmem::W4 % 16 == 0, "alignment");
+// A CTA's row of the partials buffer: the 15440 gradient sums, then its loss sum.
+constexpr int kPartStride = kNParam + 16;
 
 constexpr uint32_t kZ1 = 0, kZ2 = 64, kZ3 = 128, kDH = 128, kGW1 = 208, kGW2 = 288, kGW3 = 368;
 constexpr uint32_t kTrainCols = 512;
@@ -296,12 +298,11 @@ __global__ void __launch_bounds__(128, 1)
     k_train(const float* __restrict__ bank, int n, int count, const __nv_bfloat16* __restrict__ wb,
             const float* __restrict__ params, const Consts* __restrict__ ccp,
             const int* __restrict__ step_dev, int64_t step_override, uint64_t seed, int ntiles,
-            float inv_batch, float* __restrict__ partials, float* __restrict__ loss_ring,
-            int* __restrict__ err) {
+            float inv_batch, float* __restrict__ partials, int* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tslot;
-    __shared__ float sLoss;
+    __shared__ float sLoss[4];
     unsigned char* sW = smem + TrainSmem::W;
     unsigned char* sX = smem + TrainSmem::X;
     unsigned char* sH1 = smem + TrainSmem::H1;
@@ -315,14 +316,11 @@ __global__ void __launch_bounds__(128, 1)
     const int64_t step = step_override >= 0 ? step_override : (int64_t)*step_dev;
 
     stage_weights<128>(sW, wb);
-    if (t < kK) {
-        sW4[t] = params[kLayers * kWsz + t];
-        sDW4[t] = 0.f;
-    }
+    if (t < kK) sW4[t] = params[kLayers * kWsz + t];
+    for (int i = t; i < 4 * kK; i += blockDim.x) sDW4[i] = 0.f;  // one row per warp
     init_hidden_bias(sH1, t);
     init_hidden_bias(sH2, t);
     if (t == 0) {
-        sLoss = 0.f;
         tc::mbar_init(&bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -394,11 +392,12 @@ __global__ void __launch_bounds__(128, 1)
             }
             st_row8(sDZ, t, c, kH, dz);
             const int col = warp_sum8(z, lane);
-            if ((lane & 3) == 0) atomicAdd(&sDW4[c + col], z[0]);
+            // lanes 0, 4, .., 28 hold distinct columns: this warp's row, no atomics
+            if ((lane & 3) == 0) sDW4[warp * kK + c + col] += z[0];
         }
         {
             const float sdy = warp_sum(dy);
-            if (lane == 0) atomicAdd(&sDW4[kBiasH], sdy);
+            if (lane == 0) sDW4[warp * kK + kBiasH] += sdy;
         }
 
         // ---- backward through layers 3, 2, 1
@@ -452,7 +451,7 @@ __global__ void __launch_bounds__(128, 1)
     }
 
     if (ok) {
-        float* out = partials + (size_t)blockIdx.x * kNParam;
+        float* out = partials + (size_t)blockIdx.x * kPartStride;
         const uint32_t gw[3] = {kGW1, kGW2, kGW3};
         for (int l = 0; l < kLayers; ++l) {
 #pragma unroll 1
@@ -468,10 +467,12 @@ __global__ void __launch_bounds__(128, 1)
             }
         }
         loss = warp_sum(loss);
-        if (lane == 0) atomicAdd(&sLoss, loss);
+        if (lane == 0) sLoss[warp] = loss;
         __syncthreads();
-        if (t < kK) out[kLayers * kWsz + t] = sDW4[t];
-        if (t == 0) atomicAdd(&loss_ring[step & (kLossRing - 1)], sLoss * inv_batch);
+        // fixed summation orders throughout: the gradient and loss are bit-reproducible
+        if (t < kK) out[kLayers * kWsz + t] = ((sDW4[t] + sDW4[kK + t]) + sDW4[2 * kK + t]) +
+                                              sDW4[3 * kK + t];
+        if (t == 0) out[kNParam] = (((sLoss[0] + sLoss[1]) + sLoss[2]) + sLoss[3]) * inv_batch;
     } else if (t == 0) {
         atomicExch(err, 1);
     }
@@ -486,19 +487,22 @@ struct AdamCfg {
     int total, warmup;
 };
 
+// Sums the CTAs' partial rows in order; thread kNParam also records the step's loss and (when
+// `advance`) moves the step counter on — one thread reads and writes it.
 __global__ void k_grad_reduce(const float* __restrict__ partials, int nblk, float* __restrict__ grad,
-                              int* __restrict__ step_dev, float* __restrict__ loss_ring, int advance) {
+                              int* __restrict__ step_dev, int64_t step_override,
+                              float* __restrict__ loss_ring, int advance) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > kNParam) return;
+    float s = 0.f;
+    for (int b = 0; b < nblk; ++b) s += partials[(size_t)b * kPartStride + j];
     if (j < kNParam) {
-        float s = 0.f;
-        for (int b = 0; b < nblk; ++b) s += partials[(size_t)b * kNParam + j];
         grad[j] = s;
+        return;
     }
-    if (advance && j == 0) {
-        const int next = *step_dev + 1;
-        *step_dev = next;
-        loss_ring[next & (kLossRing - 1)] = 0.f;
-    }
+    const int64_t step = step_override >= 0 ? step_override : (int64_t)*step_dev;
+    loss_ring[step & (kLossRing - 1)] = s;
+    if (advance) *step_dev = (int)step + 1;
 }
 
 // Adam (Kingma and Ba) with a linear warm-up and cosine decay of the learning rate; step_dev
@@ -805,10 +809,10 @@ int launch_train_step(sp_closure* c, int ntiles, uint64_t seed, int64_t step_ove
     const float inv_batch = 1.f / ((float)ntiles * (float)kTile);
     k_train<<<grid, 128, TrainSmem::BYTES, st>>>(c->bank, c->n, c->count, c->wb, c->params,
                                                  c->consts_dev, c->step_dev, step_override, seed,
-                                                 ntiles, inv_batch, c->partials, c->loss, c->err);
+                                                 ntiles, inv_batch, c->partials, c->err);
     CL_CUDA(cudaGetLastError());
-    k_grad_reduce<<<(kNParam + 255) / 256, 256, 0, st>>>(c->partials, grid, c->grad, c->step_dev,
-                                                         c->loss, advance ? 1 : 0);
+    k_grad_reduce<<<(kNParam + 1 + 255) / 256, 256, 0, st>>>(
+        c->partials, grid, c->grad, c->step_dev, step_override, c->loss, advance ? 1 : 0);
     CL_CUDA(cudaGetLastError());
     c->launches += 2;
     if (adam) {
@@ -894,7 +898,7 @@ sp_closure* sp_closure_create(int n, int capacity, int* status) {
                cudaMalloc(&c->adam_m, kNParam * sizeof(float)) == cudaSuccess &&
                cudaMalloc(&c->adam_v, kNParam * sizeof(float)) == cudaSuccess &&
                cudaMalloc(&c->grad, kNParam * sizeof(float)) == cudaSuccess &&
-               cudaMalloc(&c->partials, (size_t)sms * kNParam * sizeof(float)) == cudaSuccess &&
+               cudaMalloc(&c->partials, (size_t)sms * kPartStride * sizeof(float)) == cudaSuccess &&
                cudaMalloc(&c->loss, kLossRing * sizeof(float)) == cudaSuccess &&
                cudaMalloc(&c->wb, kLayers * kWsz * sizeof(__nv_bfloat16)) == cudaSuccess &&
                cudaMalloc(&c->step_dev, sizeof(int)) == cudaSuccess &&
@@ -1085,7 +1089,6 @@ int sp_closure_grad(sp_closure* c, int64_t step, int batch_tiles, uint64_t seed,
     if (!c || step < 0 || batch_tiles < 1) return SP_ERR_ARG;
     if (c->count < 1) return cfail(c, SP_ERR_STATE, "snapshot bank is empty");
     auto st = (cudaStream_t)stream;
-    CL_CUDA(cudaMemsetAsync(c->loss + (step & (kLossRing - 1)), 0, sizeof(float), st));
     int r = launch_train_step(c, batch_tiles, seed, step, false, false, st);
     if (r) return r;
     return check_err_flag(c, st, "sp_closure_grad");
@@ -1136,6 +1139,24 @@ int sp_closure_train(sp_closure* c, int steps, int batch_tiles, uint64_t seed, v
     c->host_step += steps;
     return check_err_flag(c, st, "sp_closure_train");
 }
+
+int sp_closure_train_begin(sp_closure* c, int batch_tiles, uint64_t seed, void* stream) {
+    if (!c || batch_tiles < 1) return SP_ERR_ARG;
+    if (c->count < 1) return cfail(c, SP_ERR_STATE, "snapshot bank is empty");
+    return launch_train_step(c, batch_tiles, seed, -1, true, false, (cudaStream_t)stream);
+}
+
+int sp_closure_train_finish(sp_closure* c, void* stream) {
+    if (!c) return SP_ERR_ARG;
+    k_adam<<<(kNParam + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        c->params, c->adam_m, c->adam_v, c->grad, c->wb, c->step_dev, c->adam);
+    CL_CUDA(cudaGetLastError());
+    c->launches += 1;
+    c->host_step += 1;
+    return SP_OK;
+}
+
+void* sp_closure_grad_buffer(sp_closure* c) { return c ? (void*)c->grad : nullptr; }
 
 int64_t sp_closure_step_count(const sp_closure* c) { return c ? c->host_step : -1; }
 

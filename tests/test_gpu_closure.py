@@ -286,3 +286,19 @@ def test_closure_solver_step_matches_oracle(every_stage):
     assert np.abs(got - want).max() <= 1e-5 * scale
     # the closure changed the step by far more than that tolerance
     assert np.abs(want - plain.get_state()).max() > 50 * 1e-5 * scale
+
+
+def test_data_parallel_training_on_one_rank_is_plain_training():
+    from pyspectral_b200.sharding import train_data_parallel
+
+    n = 128
+    bank = _bank(n, 3, 90)
+    a, p = _net_with(n, bank, 7)
+    b, _ = _net_with(n, bank, 7)
+    for net in (a, b):
+        net.set_adam(lr=2e-3, lr_min=1e-4, total_steps=60, warmup=5)
+    la = a.train(60, batch_tiles=24, seed=3)  # graph-replayed chunks
+    lb = train_data_parallel(b, 60, batch_tiles=24, seed=3)  # split steps, world of one
+    np.testing.assert_array_equal(a.params(), b.params())
+    np.testing.assert_array_equal(la, lb)
+    assert a.step_count == b.step_count == 60

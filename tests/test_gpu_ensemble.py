@@ -187,3 +187,20 @@ def test_autotuner_times_candidates_and_caches(tmp_path, monkeypatch):
     again = Ensemble(cfgs, autotune=True)
     assert again.tuner.report[tune_key(gpu, 128, False, 2)]["cached"] is True
     assert again.tiles == ens.tiles
+
+
+def test_sharded_ensemble_on_one_rank_is_the_ensemble():
+    from pyspectral_b200.ensemble import Ensemble
+    from pyspectral_b200.sharding import ShardedEnsemble
+
+    cfgs = _members("float64")
+    ics = _ics(cfgs)
+    a, b = Ensemble(cfgs, autotune=False), ShardedEnsemble(cfgs, factory=lambda c: Ensemble(c, autotune=False))
+    a.set_states(ics)
+    b.set_states(ics)
+    for k in range(3):
+        dt = np.array([1e-3 * (1 + 0.1 * i + 0.05 * k) for i in range(len(cfgs))])
+        a.step(dt)
+        b.step(dt)
+    np.testing.assert_array_equal(a.diagnostics(3.0, 5.0), b.diagnostics(3.0, 5.0))
+    np.testing.assert_array_equal(a.max_velocity_sum(), b.max_velocity_sum())
