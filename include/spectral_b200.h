@@ -324,6 +324,41 @@ int sp_attach_closure(sp_solver* s, sp_closure* c);
  * solver step; synchronises `stream`. */
 int sp_closure_check(sp_closure* c, void* stream);
 
+/* ---------------------------------------------------------------- slab-decomposed 3D runs
+ * No reference counterpart (the reference runs on one device).  One run of grid n spread over
+ * nranks processes (one GPU each, nranks dividing n, m = n / nranks): rank r holds the ky slab
+ * [r m, (r+1) m) of the spectral state (per component (n, m, n/2+1), u0 layout otherwise) and
+ * the x slab [r m, (r+1) m) of the physical fields.  An RK stage is sp_slab_stage_part(0, s),
+ * an all-to-all of `send` into `recv` (nranks equal contiguous blocks of
+ * sp_slab_exchange_block_bytes(part 0) bytes; block p goes to rank p), part 1, the same
+ * exchange with part 1's block size, part 2.  Sizes (sp_slab_query_sizes, 8 entries): modes per
+ * local field, state bytes (3 fields), work bytes, send bytes (= recv bytes), aux bytes, cuFFT
+ * work bytes, m, work fields.  Every call enqueues on `stream`; sp_slab_energy and
+ * sp_slab_max_velocity synchronise it. */
+typedef struct sp_slab sp_slab;
+sp_slab* sp_slab_create(int n, int nranks, int rank, int form, int fp64, int* status);
+void sp_slab_destroy(sp_slab* s);
+const char* sp_slab_last_error(const sp_slab* s);
+int64_t sp_slab_kernel_launches(const sp_slab* s);
+int sp_slab_query_sizes(const sp_slab* s, int64_t* out, int count);
+int64_t sp_slab_exchange_block_bytes(const sp_slab* s, int part);
+/* With one rank `recv` may be `send` itself: the exchange is then nothing. */
+int sp_slab_bind(sp_slab* s, void* u0, void* acc, void* work, void* send, void* recv, void* aux,
+                 void* fft_workspace);
+int sp_slab_set_physics(sp_slab* s, double nu, double alpha, double drag_k2, double force_klo,
+                        double force_khi);
+int sp_slab_set_forcing_amplitude(sp_slab* s, double amp);
+/* Step scalars and integrating-factor table for the next step (as sp_step does). */
+int sp_slab_set_dt(sp_slab* s, double dt, void* stream);
+/* sp_prepare for the local slab: dealias u0 in place, build the stage-0 inputs. */
+int sp_slab_prepare(sp_slab* s, void* stream);
+int sp_slab_stage_part(sp_slab* s, int part, int stage, void* stream);
+/* max |u_i| of this rank's x slab of the velocity the last stage 0 transformed (the CFL bound of
+ * the state that step started from; take the max over ranks). */
+int sp_slab_max_velocity(sp_slab* s, double* out3, void* stream);
+/* Kinetic energy of this rank's slab of `state` (sum over ranks = the run's energy). */
+int sp_slab_energy(sp_slab* s, const void* state, double* out, void* stream);
+
 /* Largest number of spectrum shells sp_spectrum_noalloc accepts: its accumulators are a fixed
  * file-scope device array of this many doubles (128 KiB).  2D grids up to n = 23168 fit, and
  * every 3D grid the engine indexes with 32 bits (n <= 1290). */

@@ -102,6 +102,20 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_closure_infer": (_i, [_vp, _vp, _i64, _i, _vp, _i, _vp]),
     "sp_closure_infer_async": (_i, [_vp, _vp, _i64, _i, _vp, _i, _vp]),
     "sp_attach_closure": (_i, [_vp, _vp]),
+    "sp_slab_create": (_vp, [_i, _i, _i, _i, _i, ctypes.POINTER(_i)]),
+    "sp_slab_destroy": (None, [_vp]),
+    "sp_slab_last_error": (ctypes.c_char_p, [_vp]),
+    "sp_slab_kernel_launches": (_i64, [_vp]),
+    "sp_slab_query_sizes": (_i, [_vp, ctypes.POINTER(ctypes.c_int64), _i]),
+    "sp_slab_exchange_block_bytes": (_i64, [_vp, _i]),
+    "sp_slab_bind": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "sp_slab_set_physics": (_i, [_vp, _d, _d, _d, _d, _d]),
+    "sp_slab_set_forcing_amplitude": (_i, [_vp, _d]),
+    "sp_slab_set_dt": (_i, [_vp, _d, _vp]),
+    "sp_slab_prepare": (_i, [_vp, _vp]),
+    "sp_slab_stage_part": (_i, [_vp, _i, _i, _vp]),
+    "sp_slab_max_velocity": (_i, [_vp, _vp, _vp]),
+    "sp_slab_energy": (_i, [_vp, _vp, _vp, _vp]),
     "sp_closure_check": (_i, [_vp, _vp]),
 }
 

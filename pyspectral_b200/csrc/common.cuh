@@ -2,6 +2,8 @@
 // the device-resident parameter block and the Lawson IF-RK4 stage update.
 #pragma once
 
+#include <cmath>
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -113,6 +115,35 @@ struct StepParams {
     T ka2;         // drag acts on k^2 <= ka2
     T scale;       // 1 / n^d, folded into the inverse-FFT inputs
 };
+
+// Host side: the step scalars and the separable table, computed in fp64 and rounded to T
+// (if_table / if_scalars of src/pyspectral/backends/_fused_common.py:10-19 and the band on/off
+// rule of cupy_cuda.py:156-159).
+template <typename T>
+inline StepParams<T> make_step_params(double dt, double alpha, double amp, double klo,
+                                      double khi, double drag_k2, double scale) {
+    StepParams<T> p;
+    p.dt = (T)dt;
+    p.ea1 = (T)std::exp(-alpha * dt);
+    p.eah = (T)std::exp(-alpha * 0.5 * dt);
+    p.eb1 = (T)std::exp(amp * dt);
+    p.ebh = (T)std::exp(amp * 0.5 * dt);
+    const bool band_on = amp != 0.0;
+    p.klo2 = band_on ? (T)(klo * klo) : (T)1;
+    p.khi2 = band_on ? (T)(khi * khi) : (T)0;
+    p.ka2 = (T)drag_k2;
+    p.scale = (T)scale;
+    return p;
+}
+// tab[m] = exp(-nu m^2 dt), tab[nh + m] = exp(-nu m^2 dt / 2), m < nh
+template <typename T>
+inline void make_if_table(double nu, double dt, int nh, T* tab) {
+    for (int m = 0; m < nh; ++m) {
+        const double mm = (double)m;
+        tab[m] = (T)std::exp(-nu * mm * mm * dt);
+        tab[nh + m] = (T)std::exp(-nu * mm * mm * 0.5 * dt);
+    }
+}
 
 // Integrating factors exp(L dt) and exp(L dt/2) of one mode.  L is separable apart from the
 // drag and band indicator terms, so the viscous part is a product of 1D table entries

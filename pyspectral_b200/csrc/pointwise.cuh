@@ -206,7 +206,8 @@ __global__ void __launch_bounds__(kBlock) k_post2d(cplx<T>* __restrict__ W,
 }
 
 // --------------------------------------------------------------------------------------- 3D
-// (n, n, nh) spectral layout per component, idx = (i*n + j)*nh + l.
+// (n, n, nh) spectral layout per component, idx = (i*n + j)*nh + l; a ky slab of a distributed
+// run holds (n, ny, nh) with local index jl and global ky index j = j0 + jl.
 template <typename T>
 struct Mode3 {
     T kx, ky, kz, k2;
@@ -229,19 +230,22 @@ __device__ __forceinline__ Mode3<T> mode3(int i, int j, int l, int n) {
     return m;
 }
 
-// Walks (i, j, l) through consecutive flat indices.
+// Walks (i, jl, l) through consecutive flat indices of an (n, ny, nh) array; j() is the global
+// ky index j0 + jl (ny = n, j0 = 0 for a whole grid).
 struct Walk3 {
-    uint32_t i, j, l;
-    __device__ __forceinline__ Walk3(uint32_t idx, int n, int nh) {
+    uint32_t i, jl, l;
+    int j0;
+    __device__ __forceinline__ Walk3(uint32_t idx, int ny, int nh, int j0_) : j0(j0_) {
         uint32_t t = idx / (uint32_t)nh;
         l = idx - t * (uint32_t)nh;
-        i = t / (uint32_t)n;
-        j = t - i * (uint32_t)n;
+        i = t / (uint32_t)ny;
+        jl = t - i * (uint32_t)ny;
     }
-    __device__ __forceinline__ void next(int n, int nh) {
+    __device__ __forceinline__ int j() const { return j0 + (int)jl; }
+    __device__ __forceinline__ void next(int ny, int nh) {
         if (++l == (uint32_t)nh) {
             l = 0;
-            if (++j == (uint32_t)n) { j = 0; ++i; }
+            if (++jl == (uint32_t)ny) { jl = 0; ++i; }
         }
     }
 };
@@ -269,7 +273,8 @@ template <typename T, bool ROT>
 __global__ void __launch_bounds__(kBlock) k_pre3d(cplx<T>* __restrict__ u0,
                                                   cplx<T>* __restrict__ W, int n, int nh,
                                                   uint32_t fsc,
-                                                  const StepParams<T>* __restrict__ P) {
+                                                  const StepParams<T>* __restrict__ P,
+                                                  int ny = 0, int j0 = 0) {
     uint32_t idx0 = 2u * (blockIdx.x * blockDim.x + threadIdx.x);
     if (idx0 >= fsc) return;
     const T scale = P->scale;
@@ -277,13 +282,14 @@ __global__ void __launch_bounds__(kBlock) k_pre3d(cplx<T>* __restrict__ u0,
     ld2(u0 + idx0, a[0], a[1]);
     ld2(u0 + fsc + idx0, b[0], b[1]);
     ld2(u0 + 2 * fsc + idx0, c[0], c[1]);
-    Walk3 w(idx0, n, nh);
+    const int ly = ny ? ny : n;
+    Walk3 w(idx0, ly, nh, j0);
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
-        Mode3<T> m = mode3<T>((int)w.i, (int)w.j, (int)w.l, n);
+        Mode3<T> m = mode3<T>((int)w.i, w.j(), (int)w.l, n);
         if (!m.keep) a[e] = b[e] = c[e] = mk<T>(0, 0);
         inputs3<T, ROT>(m, scale, a[e], b[e], c[e], o[e]);
-        w.next(n, nh);
+        w.next(ly, nh);
     }
     st2(u0 + idx0, a[0], a[1]);
     st2(u0 + fsc + idx0, b[0], b[1]);
@@ -338,7 +344,7 @@ __global__ void __launch_bounds__(kBlock) k_post3d(cplx<T>* __restrict__ W,
                                                    cplx<T>* __restrict__ acc,
                                                    const T* __restrict__ tab,
                                                    const StepParams<T>* __restrict__ P, int n,
-                                                   int nh, uint32_t fsc) {
+                                                   int nh, uint32_t fsc, int ny = 0, int j0 = 0) {
     uint32_t idx0 = 2u * (blockIdx.x * blockDim.x + threadIdx.x);
     if (idx0 >= fsc) return;
     const StepParams<T> p = *P;
@@ -351,10 +357,11 @@ __global__ void __launch_bounds__(kBlock) k_post3d(cplx<T>* __restrict__ W,
         ld2(u0 + (size_t)c * fsc + idx0, U[c][0], U[c][1]);
         if (STAGE > 0) ld2(acc + (size_t)c * fsc + idx0, C[c][0], C[c][1]);
     }
-    Walk3 w(idx0, n, nh);
+    const int ly = ny ? ny : n;
+    Walk3 w(idx0, ly, nh, j0);
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
-        Mode3<T> m = mode3<T>((int)w.i, (int)w.j, (int)w.l, n);
+        Mode3<T> m = mode3<T>((int)w.i, w.j(), (int)w.l, n);
         cplx<T> N0 = mk<T>(0, 0), N1 = mk<T>(0, 0), N2 = mk<T>(0, 0);
         if (m.keep) {
             if (ROT) {
@@ -387,7 +394,7 @@ __global__ void __launch_bounds__(kBlock) k_post3d(cplx<T>* __restrict__ W,
             U[2][e] = c;
         }
         inputs3<T, ROT>(m, p.scale, a, b, c, out[e]);
-        w.next(n, nh);
+        w.next(ly, nh);
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {

@@ -145,17 +145,8 @@ unsigned grid_for(uint64_t items, int block) { return (unsigned)((items + block 
 // band on/off rule of cupy_cuda.py:156-159.
 template <typename T>
 void fill_params(sp_solver* s, double dt, std::vector<unsigned char>& out) {
-    StepParams<T> p;
-    p.dt = (T)dt;
-    p.ea1 = (T)std::exp(-s->alpha * dt);
-    p.eah = (T)std::exp(-s->alpha * 0.5 * dt);
-    p.eb1 = (T)std::exp(s->amp * dt);
-    p.ebh = (T)std::exp(s->amp * 0.5 * dt);
-    bool band_on = s->amp != 0.0;
-    p.klo2 = band_on ? (T)(s->klo * s->klo) : (T)1;
-    p.khi2 = band_on ? (T)(s->khi * s->khi) : (T)0;
-    p.ka2 = (T)s->drag_k2;
-    p.scale = (T)(1.0 / std::pow((double)s->n, (double)s->dim));
+    const StepParams<T> p = make_step_params<T>(dt, s->alpha, s->amp, s->klo, s->khi, s->drag_k2,
+                                                1.0 / std::pow((double)s->n, (double)s->dim));
     out.resize(sizeof(p));
     std::memcpy(out.data(), &p, sizeof(p));
 }
@@ -163,11 +154,7 @@ void fill_params(sp_solver* s, double dt, std::vector<unsigned char>& out) {
 template <typename T>
 void fill_table(sp_solver* s, double dt, std::vector<unsigned char>& out) {
     std::vector<T> t(2 * (size_t)s->nh);
-    for (int m = 0; m < s->nh; ++m) {
-        double mm = (double)m;
-        t[m] = (T)std::exp(-s->nu * mm * mm * dt);
-        t[s->nh + m] = (T)std::exp(-s->nu * mm * mm * 0.5 * dt);
-    }
+    make_if_table<T>(s->nu, dt, s->nh, t.data());
     out.resize(t.size() * sizeof(T));
     std::memcpy(out.data(), t.data(), out.size());
 }

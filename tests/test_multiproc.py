@@ -170,3 +170,33 @@ def test_gradient_mean_over_two_ranks():
         assert r.returncode == 0, r.stderr
     for o in (json.loads(r.stdout.strip().splitlines()[-1]) for r in res):
         assert o["lo"] == o["hi"] == 1.5
+
+
+EXCHANGE_WORKER = r"""
+import json, os, sys, datetime
+sys.path.insert(0, {root!r})
+import torch, torch.distributed as dist
+from pyspectral_b200.slab import exchange_blocks
+dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+r, P, nb = dist.get_rank(), dist.get_world_size(), 6
+send = torch.zeros(P * nb + 5, dtype=torch.uint8)   # spare tail bytes stay untouched
+for p in range(P):
+    send[p * nb:(p + 1) * nb] = 10 * r + p             # block p is for rank p
+recv = torch.full((P * nb + 5,), 255, dtype=torch.uint8)
+exchange_blocks(recv, send, nb, P, dist)
+dist.destroy_process_group()
+print(json.dumps({{"rank": r, "recv": recv.tolist()}}))
+"""
+
+
+def test_slab_exchange_block_convention():
+    import json
+
+    res = _launch(EXCHANGE_WORKER.format(root=str(ROOT)))
+    for r in res:
+        assert r.returncode == 0, r.stderr
+    for o in (json.loads(r.stdout.strip().splitlines()[-1]) for r in res):
+        me, nb = o["rank"], 6
+        for src in range(2):  # block `src` of my recv came from rank src, aimed at me
+            assert o["recv"][src * nb:(src + 1) * nb] == [10 * src + me] * nb
+        assert o["recv"][2 * nb:] == [255] * 5
