@@ -490,8 +490,8 @@ def ours_closure(args, w: dict) -> int:
                      "traffic": None, "flop_per_launch": flop, "launch_ms": t_inf},
         "e2e": {"value": ev["wall_ratio"], "unit": "x", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0,
-                "what": "wall clock of simulate.run (CFL and forcing control, host driven) to "
-                        "t_end for both runs"},
+                "what": "wall clock of simulate.run_device (CFL and constant-power control on "
+                        "the device, one host read per 10 steps) to t_end for both runs"},
         "gpu_launches": int(net.kernel_launches), "clocks": clk,
     }
     print(json.dumps(line), flush=True)

@@ -359,6 +359,19 @@ int sp_slab_max_velocity(sp_slab* s, double* out3, void* stream);
 /* Kinetic energy of this rank's slab of `state` (sum over ranks = the run's energy). */
 int sp_slab_energy(sp_slab* s, const void* state, double* out, void* stream);
 
+/* ---------------------------------------------------------------- device-run loop
+ * simulate.run's loop (src/pyspectral/simulate.py:45-95, without records or callbacks) with its
+ * control on the GPU: every cfl_every steps the CFL bound and, when target_power >= 0, the
+ * constant-power amplitude A = P / (2 E_band) come from device reductions of the live state;
+ * every step dt = min(h, t_end - t) and the step scalars and integrating-factor table are
+ * written by a one-block kernel.  Chunks of cfl_every steps replay one captured graph; the host
+ * reads t back once per chunk.  dt_fixed > 0 replaces the CFL rule by a fixed step.  *t_io: the
+ * run's start time in, end time out; stops at t_end or after max_steps steps (steps of the last
+ * chunk past t_end have dt = 0 and leave the state unchanged). */
+int sp_run_to(sp_solver* s, double t_end, double cfl, double dt_max, int cfl_every,
+              double target_power, double dt_fixed, int64_t max_steps, double* t_io,
+              int64_t* steps_out, double* amp_out, void* stream);
+
 /* Largest number of spectrum shells sp_spectrum_noalloc accepts: its accumulators are a fixed
  * file-scope device array of this many doubles (128 KiB).  2D grids up to n = 23168 fit, and
  * every 3D grid the engine indexes with 32 bits (n <= 1290). */

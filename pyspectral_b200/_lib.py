@@ -102,6 +102,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_closure_infer": (_i, [_vp, _vp, _i64, _i, _vp, _i, _vp]),
     "sp_closure_infer_async": (_i, [_vp, _vp, _i64, _i, _vp, _i, _vp]),
     "sp_attach_closure": (_i, [_vp, _vp]),
+    "sp_run_to": (_i, [_vp, _d, _d, _d, _i, _d, _d, _i64, _dp, ctypes.POINTER(_i64), _dp, _vp]),
     "sp_slab_create": (_vp, [_i, _i, _i, _i, _i, ctypes.POINTER(_i)]),
     "sp_slab_destroy": (None, [_vp]),
     "sp_slab_last_error": (ctypes.c_char_p, [_vp]),

@@ -327,13 +327,22 @@ class ClosureSolver(B200Solver):
         self._mode: bool | None = None  # update mode the step graph was captured with
         super().__init__(cfg)
 
-    def _step(self, dt: float) -> None:
+    def run_to(self, t_end: float, **kw: Any) -> int:
+        self._sync_mode()
+        n = super().run_to(t_end, **kw)
+        self.net.check()
+        return n
+
+    def _sync_mode(self) -> None:
         if self._mode != self.every_stage or self.net.every_stage != self.every_stage:
             # the closure object is shared: set its mode and re-capture this solver's graph
             self.net.set_update(self.every_stage)
             self._check(self.lib.sp_set_graph(self._h, 0), "sp_set_graph")
             self._check(self.lib.sp_set_graph(self._h, int(self.use_graph)), "sp_set_graph")
             self._mode = self.every_stage
+
+    def _step(self, dt: float) -> None:
+        self._sync_mode()
         super()._step(dt)
 
     def _before_bind(self, h: int) -> None:

@@ -252,14 +252,16 @@ def _record_run(solver: Any, meter: FluxMeter, nl_of: Any, sc: StudyConfig) -> R
 
 
 def _timed_run(solver: Any, state: Any, sc: StudyConfig) -> tuple[float, int]:
-    """Wall time of one run to t_eval (CFL and forcing control included); the step graph is
-    captured by an untimed step first."""
+    """Wall time of one run to t_eval with the run loop's control on the device (CFL and
+    constant-power forcing every 10 steps, simulate.run_device); the chunk graph is captured by
+    a short untimed run first."""
     solver.set_state(state)
-    solver.step(1e-6)
+    solver.run_to(1e-6, cfl=sc.cfl, dt_max=sc.dt_max, target_power=sc.power)
     solver.set_state(state)
     solver.t = 0.0
     solver.synchronize()
-    res = simulate.run(solver, sc.t_eval, cfl=sc.cfl, dt_max=sc.dt_max, target_power=sc.power)
+    res = simulate.run_device(solver, sc.t_eval, cfl=sc.cfl, dt_max=sc.dt_max,
+                              target_power=sc.power)
     return res.wall, res.steps
 
 

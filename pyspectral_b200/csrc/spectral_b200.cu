@@ -58,6 +58,17 @@ namespace sp {
 void set_thread_error(const char* why) { g_create_error = why; }
 }  // namespace sp
 
+// Device-resident run control (sp_run_to): the simulate.run rules evaluated on the GPU.
+struct RunCtl {
+    double t, t_end, tol, cfl, dt_max, dx, power, dt_fixed;
+    double h_cfl;    // step of the current CFL window
+    double dt_last;  // step just taken (t advances by it at the next control)
+    double dt_tab;   // step the integrating-factor table was last filled for
+    double amp;      // forcing amplitude in use
+    long long steps;
+    int have_power, pad;
+};
+
 struct sp_solver {
     // grid
     int n = 0, dim = 0, form = 0, fp64 = 0, fft_mode = 0;
@@ -97,6 +108,13 @@ struct sp_solver {
     bool graph_on = false;
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // device-run chunk graph (sp_run_to): cfl_every steps with their control kernels
+    cudaGraphExec_t run_exec = nullptr;
+    int run_every = 0, run_flags = -1;
+    int64_t run_kernels = 0;        // own kernels per chunk replay
+    double run_phys[5] = {0, 0, 0, 0, 0};  // nu, alpha, drag_k2, klo, khi baked into the chunk
+    size_t off_ctl = 0;
+    RunCtl host_ctl{};
     // last error
     std::string err;
 
@@ -415,6 +433,211 @@ void drop_graph(sp_solver* s) {
         cudaGraphExecDestroy(s->exec);
         s->exec = nullptr;
     }
+    if (s->run_exec) {
+        cudaGraphExecDestroy(s->run_exec);
+        s->run_exec = nullptr;
+    }
+}
+
+// ---------------------------------------------------------------------------- device runs
+// One control per step: t advances by the previous step; at a CFL step (refresh) the CFL bound
+// sum_i max|u_i| and the forcing band energy of the live state give h = min(dt_max,
+// cfl dx / umax) and A = P / (2 E_band) (simulate.run, simulate.py:45-95); then dt = min(h,
+// t_end - t) (0 once t_end is reached: the step leaves the state unchanged) and the step
+// scalars and the integrating-factor table are written for it.
+template <typename T>
+__global__ void __launch_bounds__(256) k_control(RunCtl* __restrict__ c,
+                                                 const unsigned long long* __restrict__ umax,
+                                                 int ncomp, const double* __restrict__ band,
+                                                 int refresh, StepParams<T>* __restrict__ P,
+                                                 T* __restrict__ tab, int nh, double nu,
+                                                 double alpha, double klo, double khi,
+                                                 double drag_k2, double scale) {
+    __shared__ double s_dt;
+    __shared__ int s_fill;
+    if (threadIdx.x == 0) {
+        c->t += c->dt_last;
+        if (c->dt_last > 0.0) c->steps += 1;
+        if (refresh) {
+            double h = c->dt_max;
+            if (c->dt_fixed > 0.0) {
+                h = c->dt_fixed;
+            } else {
+                double u = 0.0;
+                for (int k = 0; k < ncomp; ++k) u += __longlong_as_double((long long)umax[k]);
+                if (u > 0.0 && isfinite(u)) h = fmin(c->dt_max, c->cfl * c->dx / u);
+            }
+            c->h_cfl = h;
+            if (c->have_power) {
+                const double eb = band[3];
+                c->amp = eb > 0.0 ? c->power / (2.0 * eb) : 0.0;
+            }
+        }
+        const double dt = c->t < c->t_end - c->tol ? fmin(c->h_cfl, c->t_end - c->t) : 0.0;
+        c->dt_last = dt;
+        StepParams<T> p;
+        p.dt = (T)dt;
+        p.ea1 = (T)exp(-alpha * dt);
+        p.eah = (T)exp(-alpha * 0.5 * dt);
+        p.eb1 = (T)exp(c->amp * dt);
+        p.ebh = (T)exp(c->amp * 0.5 * dt);
+        const bool band_on = c->amp != 0.0;
+        p.klo2 = band_on ? (T)(klo * klo) : (T)1;
+        p.khi2 = band_on ? (T)(khi * khi) : (T)0;
+        p.ka2 = (T)drag_k2;
+        p.scale = (T)scale;
+        *P = p;
+        s_fill = dt != c->dt_tab;
+        c->dt_tab = dt;
+        s_dt = dt;
+    }
+    __syncthreads();
+    if (!s_fill) return;
+    const double dt = s_dt;
+    for (int m = threadIdx.x; m < nh; m += blockDim.x) {
+        const double mm = (double)m;
+        tab[m] = (T)exp(-nu * mm * mm * dt);
+        tab[nh + m] = (T)exp(-nu * mm * mm * 0.5 * dt);
+    }
+}
+
+__global__ void k_control_close(RunCtl* __restrict__ c) {
+    c->t += c->dt_last;
+    if (c->dt_last > 0.0) c->steps += 1;
+    c->dt_last = 0.0;
+}
+
+}  // namespace
+
+namespace {
+
+// The CFL bound and the band energy of the live state, enqueued without a host read:
+// umax_dev()[0..ncomp) and out_dev()[3].
+int enqueue_run_diag(sp_solver* s, bool need_umax, bool need_band, cudaStream_t st) {
+    if (need_umax) {
+        SP_CUDA(cudaMemsetAsync(s->umax_dev(), 0, 4 * sizeof(unsigned long long), st));
+        if (s->fused()) {
+            SP_CUDA(sp::fused::row_max(s->n, s->fp64, s->W, s->kc, s->tw_dev(), s->umax_dev(), st));
+            s->launches += 1;
+        } else {
+            cufftHandle plan = s->fft_mode == SP_FFT_CUFFT_LEAN ? s->plan_inv : s->plan_c2r1;
+            unsigned gv = grid_for(s->fsc, kRedThreads);
+            uint32_t rows = s->fsc / (uint32_t)s->nh;
+            unsigned gm = grid_for((uint64_t)rows * (s->n / 2), kRedThreads);
+            if (gm > (unsigned)kRedBlocks) gm = kRedBlocks;
+            double scale = 1.0 / std::pow((double)s->n, (double)s->dim);
+            for (int c = 0; c < s->dim; ++c) {
+                if (s->fp64)
+                    k_velocity_component<double><<<gv, kRedThreads, 0, st>>>(
+                        (const cplx<double>*)s->u0, (cplx<double>*)s->acc, s->n, s->nh, s->dim,
+                        s->fsc, c, scale);
+                else
+                    k_velocity_component<float><<<gv, kRedThreads, 0, st>>>(
+                        (const cplx<float>*)s->u0, (cplx<float>*)s->acc, s->n, s->nh, s->dim,
+                        s->fsc, c, (float)scale);
+                SP_CUDA(cudaGetLastError());
+                int r = exec_c2r(s, plan, s->acc, st);
+                if (r) return r;
+                if (s->fp64)
+                    k_max_abs_padded<double><<<gm, kRedThreads, 0, st>>>(
+                        (const double*)s->acc, s->n, 2 * s->nh, rows, s->umax_dev() + c);
+                else
+                    k_max_abs_padded<float><<<gm, kRedThreads, 0, st>>>(
+                        (const float*)s->acc, s->n, 2 * s->nh, rows, s->umax_dev() + c);
+                SP_CUDA(cudaGetLastError());
+                s->launches += 2;
+            }
+        }
+    }
+    if (need_band) {
+        if (s->fused()) {
+            SP_CUDA(sp::fused::reduce_t(s->fp64, s->u0t_dev(), s->n, s->kc, 0, 1, s->klo, s->khi,
+                                        s->partials_dev(), kRedBlocks, s->out_dev(), st));
+            s->launches += 2;
+        } else {
+            double norm = std::pow((double)s->n, 2.0 * s->dim);
+            unsigned g = grid_for(s->fsc, kRedThreads);
+            if (g > (unsigned)kRedBlocks) g = kRedBlocks;
+            if (s->fp64)
+                k_reduce_spectral<double><<<g, kRedThreads, 0, st>>>(
+                    (const cplx<double>*)s->u0, s->n, s->nh, s->dim, s->fsc, 1.0 / norm,
+                    2.0 / norm, s->klo * s->klo, s->khi * s->khi, s->partials_dev());
+            else
+                k_reduce_spectral<float><<<g, kRedThreads, 0, st>>>(
+                    (const cplx<float>*)s->u0, s->n, s->nh, s->dim, s->fsc, 1.0 / norm,
+                    2.0 / norm, s->klo * s->klo, s->khi * s->khi, s->partials_dev());
+            SP_CUDA(cudaGetLastError());
+            k_finish_sum<4><<<1, kRedThreads, 0, st>>>(s->partials_dev(), (int)g, 0.5, s->out_dev());
+            SP_CUDA(cudaGetLastError());
+            s->launches += 2;
+        }
+    }
+    return SP_OK;
+}
+
+template <typename T>
+int enqueue_control(sp_solver* s, bool refresh, cudaStream_t st) {
+    k_control<T><<<1, 256, 0, st>>>((RunCtl*)((char*)s->aux + s->off_ctl), s->umax_dev(), s->dim,
+                                    s->out_dev(), refresh ? 1 : 0,
+                                    (StepParams<T>*)s->params_dev(), (T*)s->tab_dev(), s->nh,
+                                    s->nu, s->alpha, s->klo, s->khi, s->drag_k2,
+                                    1.0 / std::pow((double)s->n, (double)s->dim));
+    SP_CUDA(cudaGetLastError());
+    s->launches += 1;
+    return SP_OK;
+}
+
+// One chunk of `every` steps: at its first step the CFL / forcing refresh (when asked for),
+// then per step a control and the step; t closed at the end.
+int enqueue_run_chunk(sp_solver* s, int every, bool cfl, bool power, cudaStream_t st) {
+    int r;
+    for (int k = 0; k < every; ++k) {
+        const bool refresh = k == 0;
+        if (refresh && (r = enqueue_run_diag(s, cfl, power, st))) return r;
+        if ((r = s->fp64 ? enqueue_control<double>(s, refresh, st)
+                         : enqueue_control<float>(s, refresh, st)))
+            return r;
+        if ((r = run_step(s, st))) return r;
+    }
+    k_control_close<<<1, 1, 0, st>>>((RunCtl*)((char*)s->aux + s->off_ctl));
+    SP_CUDA(cudaGetLastError());
+    s->launches += 1;
+    return SP_OK;
+}
+
+int capture_run_chunk(sp_solver* s, int every, int flags) {
+    const double phys[5] = {s->nu, s->alpha, s->drag_k2, s->klo, s->khi};
+    if (s->run_exec && s->run_every == every && s->run_flags == flags &&
+        std::memcmp(phys, s->run_phys, sizeof(phys)) == 0)
+        return SP_OK;
+    if (s->run_exec) {
+        cudaGraphExecDestroy(s->run_exec);
+        s->run_exec = nullptr;
+    }
+    if (!s->cap_stream) SP_CUDA(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
+    SP_CUDA(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = s->launches;
+    int r = enqueue_run_chunk(s, every, flags & 1, flags & 2, s->cap_stream);
+    const int64_t per_chunk = s->launches - before;
+    s->launches = before;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->cap_stream, &g);
+    if (r) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return fail(s, SP_ERR_CUDA, "cudaStreamEndCapture", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&s->run_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        s->run_exec = nullptr;
+        return fail(s, SP_ERR_CUDA, "cudaGraphInstantiate", cudaGetErrorString(e));
+    }
+    s->run_every = every;
+    s->run_flags = flags;
+    s->run_kernels = per_chunk;
+    std::memcpy(s->run_phys, phys, sizeof(phys));
+    return SP_OK;
 }
 
 }  // namespace
@@ -481,6 +704,7 @@ sp_solver* sp_create(int n, int dim, int form, int fp64, int fft_mode, int* stat
     s->off_umax = off; off += align256(4 * sizeof(unsigned long long));
     s->off_out = off; off += align256(8 * sizeof(double));
     s->off_spec = off; off += align256((size_t)s->nshell * sizeof(double));
+    s->off_ctl = off; off += align256(sizeof(RunCtl));
     s->off_tw = off;
     if (fft_mode == SP_FFT_FUSED && sp::fused::supported(n, fp64))
         off += align256((size_t)sp::fused::twiddle_table_size(n) * 2 * s->rsize);
@@ -886,6 +1110,55 @@ int sp_nonlinear(sp_solver* s, const void* state, void* out, void* stream) {
     s->launches += 3;
     // the work array held the next stage's inputs: rebuild them from the state
     return run_pre(s, st);
+}
+
+int sp_run_to(sp_solver* s, double t_end, double cfl, double dt_max, int cfl_every,
+              double target_power, double dt_fixed, int64_t max_steps, double* t_io,
+              int64_t* steps_out, double* amp_out, void* stream) {
+    SP_CHECK_BOUND(s);
+    if (!t_io || cfl_every < 1 || cfl_every > 1000 || !(dt_max > 0.0) || max_steps < 0)
+        return fail(s, SP_ERR_ARG, "sp_run_to", "bad arguments");
+    auto st = (cudaStream_t)stream;
+    const bool use_cfl = !(dt_fixed > 0.0);
+    const bool use_power = target_power >= 0.0;
+    const int flags = (use_cfl ? 1 : 0) | (use_power ? 2 : 0) |
+                      ((s->cl() && sp::closure::every_stage(s->closure)) ? 4 : 0);
+    // the step graph and the chunk graph share the device parameter block
+    int r = capture_run_chunk(s, cfl_every, flags);
+    if (r) return r;
+    const int64_t per_chunk = s->run_kernels;
+    RunCtl& c = s->host_ctl;
+    c = RunCtl{};
+    c.t = *t_io;
+    c.t_end = t_end;
+    c.tol = 1e-12 * std::max(1.0, t_end);
+    c.cfl = cfl;
+    c.dt_max = dt_max;
+    c.dx = 2.0 * M_PI / (double)s->n;
+    c.power = use_power ? target_power : 0.0;
+    c.dt_fixed = use_cfl ? 0.0 : dt_fixed;
+    c.dt_tab = -1.0;
+    c.amp = s->amp;
+    c.have_power = use_power ? 1 : 0;
+    RunCtl* dc = (RunCtl*)((char*)s->aux + s->off_ctl);
+    SP_CUDA(cudaMemcpyAsync(dc, &c, sizeof(RunCtl), cudaMemcpyHostToDevice, st));
+    if (s->fused()) s->u0_fresh = false;
+    int64_t chunks = 0;
+    while (c.t < t_end - c.tol && c.steps < max_steps) {
+        SP_CUDA(cudaGraphLaunch(s->run_exec, st));
+        s->launches += per_chunk;
+        ++chunks;
+        SP_CUDA(cudaMemcpyAsync(&c, dc, sizeof(RunCtl), cudaMemcpyDeviceToHost, st));
+        SP_CUDA(cudaStreamSynchronize(st));
+    }
+    // the host-side caches of the step scalars no longer describe the device block
+    s->params_valid = false;
+    s->tab_valid = false;
+    s->amp = c.amp;
+    *t_io = c.t;
+    if (steps_out) *steps_out = c.steps;
+    if (amp_out) *amp_out = c.amp;
+    return SP_OK;
 }
 
 }  // extern "C"

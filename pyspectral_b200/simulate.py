@@ -112,3 +112,31 @@ def run_steps(solver: Any, nsteps: int, *, cfl: float = 0.5, dt_max: float = 0.0
         solver.step(h)
         dts.append(h)
     return dts
+
+
+def run_device(solver: Any, t_end: float, *, dt: float | None = None, cfl: float = 0.5,
+               dt_max: float = 0.05, cfl_every: int = 10,
+               target_power: float | None = None) -> RunResult:
+    """:func:`run` without records or callbacks, its loop control on the device
+    (``solver.run_to``: CFL bound and forcing amplitude from device reductions, one graph replay
+    per ``cfl_every`` steps, one host read per replay).  Same rules, same dt sequence; the
+    result holds the start and end records only."""
+    res = RunResult()
+    diag = solver.diag
+
+    def record() -> None:
+        st = solver.state_native()
+        res.t.append(solver.t)
+        res.energy.append(diag.energy(st))
+        res.enstrophy.append(diag.enstrophy(st))
+
+    record()
+    solver.synchronize()
+    start = time.perf_counter()
+    res.steps = solver.run_to(t_end, cfl=cfl, dt_max=dt_max, cfl_every=cfl_every,
+                              target_power=target_power, dt=dt)
+    solver.synchronize()
+    res.wall = time.perf_counter() - start
+    res.finished = solver.t >= t_end - 1e-12 * max(1.0, t_end)
+    record()
+    return res

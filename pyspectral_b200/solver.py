@@ -183,6 +183,26 @@ class B200Solver(SpectralSolver):
     def _step(self, dt: float) -> None:
         self._check(self.lib.sp_step(self._h, float(dt), self._stream()), "sp_step")
 
+    def run_to(self, t_end: float, *, cfl: float = 0.5, dt_max: float = 0.05,
+               cfl_every: int = 10, target_power: float | None = None, dt: float | None = None,
+               max_steps: int = 1 << 62) -> int:
+        """simulate.run's loop to ``t_end`` with its control on the device (sp_run_to): CFL
+        bound and constant-power amplitude every ``cfl_every`` steps from device reductions,
+        dt = min(h, t_end - t) per step, chunks of ``cfl_every`` steps replayed from one graph.
+        Returns the number of steps taken."""
+        t = ctypes.c_double(self.t)
+        steps = ctypes.c_int64(0)
+        amp = ctypes.c_double(self.force_amp)
+        self._check(self.lib.sp_run_to(
+            self._h, float(t_end), float(cfl), float(dt_max), int(cfl_every),
+            -1.0 if target_power is None else float(target_power), float(dt or 0.0),
+            int(max_steps), ctypes.byref(t), ctypes.byref(steps), ctypes.byref(amp),
+            self._stream()), "sp_run_to")
+        self.t = t.value
+        self.nstep += int(steps.value)
+        self.force_amp = amp.value
+        return int(steps.value)
+
     def run_phase(self, phase: int, stage: int = 0) -> None:
         """One phase of one stage by itself (0 inverse FFT, 1 phys, 2 forward FFT, 3 post)."""
         self._check(self.lib.sp_run_phase(self._h, int(phase), int(stage), self._stream()),
