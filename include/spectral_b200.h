@@ -134,6 +134,20 @@ int sp_sync_state(sp_solver* s, void* stream);
 /* 1 = replay each step from a CUDA graph (variant fused-inplace-graph), 0 = plain launches. */
 int sp_set_graph(sp_solver* s, int enable);
 
+/* Column pass of the fused 2D engine (SP_FFT_FUSED), process-wide: 1 (default) = the streamed
+ * persistent pass for single runs of n = 2048..8192 (fp64 up to 4096) — each CTA loops over
+ * columns and prefetches the next column's work data into shared memory by TMA while it
+ * transforms the current one; 0 = one column per CTA.  Both give the same results to round-off.
+ * Affects launches made (and graphs captured) after the call.  No reference counterpart. */
+int sp_set_column_streaming(int enable);
+int sp_column_streaming(void);
+
+/* Error bits raised by this library's kernels on the current device since the last call (then
+ * cleared) into *bits: 1 = a streamed column pass gave up waiting for its TMA data and skipped
+ * its columns (results invalid).  Synchronous; SP_ERR_CUDA if the read fails.  No reference
+ * counterpart. */
+int sp_take_device_error(unsigned int* bits);
+
 /* Spectral reductions of a state array (device pointer in the u0 layout, e.g. u0 itself):
  * writes SP_DIAG_COUNT doubles to out (host) — energy, enstrophy, palinstrophy and the energy in
  * band_klo <= |k| <= band_khi — summed in fp64 in a fixed order.  Synchronises `stream`. */

@@ -42,6 +42,9 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_step": (_i, [_vp, _d, _vp]),
     "sp_sync_state": (_i, [_vp, _vp]),
     "sp_set_graph": (_i, [_vp, _i]),
+    "sp_set_column_streaming": (_i, [_i]),
+    "sp_column_streaming": (_i, []),
+    "sp_take_device_error": (_i, [ctypes.POINTER(ctypes.c_uint)]),
     "sp_diagnostics": (_i, [_vp, _vp, _d, _d, _dp, _vp]),
     "sp_max_velocity": (_i, [_vp, _vp, _dp, _dp, _vp]),
     "sp_spectrum": (_i, [_vp, _vp, _dp, _i, _vp]),
@@ -159,3 +162,15 @@ def check(lib: ctypes.CDLL, handle: int | None, status: int, what: str) -> None:
 def dptr(arr: Any) -> ctypes.c_void_p:
     """Device pointer of a torch tensor (or None)."""
     return ctypes.c_void_p(arr.data_ptr()) if arr is not None else ctypes.c_void_p(0)
+
+
+def check_device_errors(lib: ctypes.CDLL) -> None:
+    """Raise EngineError when a kernel of this library flagged a device-side error (bounded
+    wait that gave up) since the last check; clears the flags.  Synchronous."""
+    bits = ctypes.c_uint(0)
+    st = lib.sp_take_device_error(ctypes.byref(bits))
+    if st != 0:
+        raise EngineError(f"sp_take_device_error failed: {STATUS_NAMES.get(st, st)}")
+    if bits.value:
+        raise EngineError(f"device error bits {bits.value:#x}: a streamed column pass timed out "
+                          "waiting for its TMA data; the state is invalid")

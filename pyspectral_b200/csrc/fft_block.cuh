@@ -353,6 +353,61 @@ __device__ __forceinline__ void block_fft(E (&v)[16], E* sm, int t, const C* __r
     }
 }
 
+// Exchange between two passes of a Pair transform through a buffer of single complex values
+// (half the bytes of a Pair buffer): the `a` sequences move first, then the `b` sequences.
+template <int N, int R0, int S0, int R1, typename T>
+__device__ __forceinline__ void exchange_halves(Pair<T> (&v)[16], cplx<T>* sm, int t) {
+    constexpr int G0 = 16 / R0, G1 = 16 / R1;
+    constexpr int TT = N / 16;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+#pragma unroll
+        for (int g = 0; g < G0; ++g) {
+            const int j = t + TT * g;
+            const int base = (j / S0) * S0 * R0 + (j & (S0 - 1));
+#pragma unroll
+            for (int m = 0; m < R0; ++m)
+                sm[spad(base + m * S0)] = h == 0 ? v[g * R0 + m].a : v[g * R0 + m].b;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int g = 0; g < G1; ++g)
+#pragma unroll
+            for (int m = 0; m < R1; ++m) {
+                const cplx<T> e = sm[spad(in_pos<N, R1>(t, g, m))];
+                if (h == 0) v[g * R1 + m].a = e;
+                else v[g * R1 + m].b = e;
+            }
+        __syncthreads();
+    }
+}
+
+// block_fft of Pair elements with the exchanges of exchange_halves: `sm` holds
+// FftPlan<N>::SMEM complex values instead of Pairs.
+template <int N, bool INV, typename T, typename C>
+__device__ __forceinline__ void block_fft_halves(Pair<T> (&v)[16], cplx<T>* sm, int t,
+                                                 const C* __restrict__ tw) {
+    using P = FftPlan<N>;
+    constexpr int DIR = INV ? 1 : -1;
+    constexpr int R0 = P::radix(INV, 0), S0 = P::stride(INV, 0);
+    pass_compute<N, R0, S0, DIR>(v, t, tw);
+    if constexpr (P::NP > 1) {
+        constexpr int R1 = P::radix(INV, 1), S1 = P::stride(INV, 1);
+        exchange_halves<N, R0, S0, R1>(v, sm, t);
+        pass_compute<N, R1, S1, DIR>(v, t, tw + P::tw_offset(INV, 1));
+        if constexpr (P::NP > 2) {
+            constexpr int R2 = P::radix(INV, 2), S2 = P::stride(INV, 2);
+            exchange_halves<N, R1, S1, R2>(v, sm, t);
+            pass_compute<N, R2, S2, DIR>(v, t, tw + P::tw_offset(INV, 2));
+            if constexpr (P::NP > 3) {
+                constexpr int R3 = P::radix(INV, 3), S3 = P::stride(INV, 3);
+                exchange_halves<N, R2, S2, R3>(v, sm, t);
+                pass_compute<N, R3, S3, DIR>(v, t, tw + P::tw_offset(INV, 3));
+            }
+        }
+    }
+}
+
 // radix of the last pass (output pattern) and of the first pass (input pattern)
 template <int N, bool INV>
 constexpr int first_radix() { return FftPlan<N>::radix(INV, 0); }

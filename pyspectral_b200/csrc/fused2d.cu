@@ -1,4 +1,7 @@
 // Launchers of the fused 2D engine: runtime grid size -> compile-time kernel instantiation.
+#include <cuda.h>
+
+#include <atomic>
 #include <cmath>
 
 #include "fused2d.h"
@@ -7,7 +10,95 @@
 namespace sp {
 namespace fused {
 
+// Error bits of the streamed column pass (kStreamTimeout), one word per device context.
+__device__ unsigned g_stream_err;
+
 namespace {
+
+std::atomic<bool> g_streaming{true};
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime (no link to
+// libcuda); null when the driver does not provide it.
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encoder() {
+    static const EncodeTiled fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (EncodeTiled) nullptr;
+        return (EncodeTiled)f;
+    }();
+    return fn;
+}
+
+// Tensor map of the work array X for the streamed column pass: float32 words, row q = row pair
+// q (kc * 2 Pairs), box = one column's 2 Pairs x up to 256 row pairs.
+template <typename T, int N>
+bool x_map(CUtensorMap* map, void* X, int kc) {
+    const EncodeTiled enc = encoder();
+    if (!enc || ((uintptr_t)X & 15)) return false;
+    const cuuint64_t words = (cuuint64_t)kc * 2 * sizeof(Pair<T>) / 4;
+    const cuuint64_t dims[2] = {words, (cuuint64_t)(N / 2)};
+    const cuuint64_t strides[1] = {words * 4};  // bytes between row pairs
+    const cuuint32_t box[2] = {(cuuint32_t)stream_box_w<T>(), (cuuint32_t)stream_box_h<N>()};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, X, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Grids the streamed column pass is built for: 2048..8192 (fp64 up to 4096).
+template <typename T, int N>
+constexpr bool stream_ok() { return N >= 2048 && (sizeof(T) == 4 ? N <= 8192 : N <= 4096); }
+
+// Launch facts of the streamed pass, gathered by set_attributes (outside any stream capture):
+// resident CTAs per SM for each stage, the SM count and this device's error word.
+constexpr int kMaxDevices = 64;
+unsigned* g_err_addr[kMaxDevices];
+
+template <typename T, int N>
+struct StreamLaunch {
+    static inline int per_sm[4] = {0, 0, 0, 0};
+    static inline int nsm = 0;
+};
+
+template <typename T, int N, int STAGE>
+cudaError_t stream_prepare(int n_sm) {
+    using CS = ColStream<T, N>;
+    cudaError_t e = cudaFuncSetAttribute(k_col_stream<T, N, STAGE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)CS::SMEM);
+    if (e) return e;
+    int occ = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_col_stream<T, N, STAGE>,
+                                                           CS::THREADS, CS::SMEM)))
+        return e;
+    StreamLaunch<T, N>::per_sm[STAGE] = occ;
+    StreamLaunch<T, N>::nsm = n_sm;
+    return cudaSuccess;
+}
+
+template <typename T, int N>
+cudaError_t stream_attrs() {
+    int dev = 0, n_sm = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) ||
+        (e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev)))
+        return e;
+    if (dev < kMaxDevices && !g_err_addr[dev]) {
+        if ((e = cudaGetSymbolAddress((void**)&g_err_addr[dev], g_stream_err))) return e;
+    }
+    encoder();  // resolve the driver entry point now
+    if ((e = stream_prepare<T, N, 0>(n_sm)) || (e = stream_prepare<T, N, 1>(n_sm)) ||
+        (e = stream_prepare<T, N, 2>(n_sm)) || (e = stream_prepare<T, N, 3>(n_sm)))
+        return e;
+    return cudaSuccess;
+}
 
 // Tile multipliers compiled for a grid: 1, 2, 4 up to n = 1024 (CTAs of at most 256 threads),
 // 1 above.
@@ -51,7 +142,11 @@ cudaError_t attrs() {
         return e;
     if ((e = attrs_tile<T, N, 1>())) return e;
     if ((e = attrs_tile<T, N, 2>())) return e;
-    return attrs_tile<T, N, 4>();
+    if ((e = attrs_tile<T, N, 4>())) return e;
+    if constexpr (stream_ok<T, N>()) {
+        if ((e = stream_attrs<T, N>())) return e;
+    }
+    return cudaSuccess;
 }
 
 template <typename T, int N, int BX>
@@ -103,11 +198,37 @@ struct ColArgs {
     int tile;
 };
 
+// One persistent CTA per resident slot (SM count x CTAs per SM), at most one per column.
+// Returns false (nothing launched) when the pass was not prepared for this device.
+template <typename T, int N, int STAGE>
+bool col_stream(const ColArgs& a, const CUtensorMap& map, cudaError_t* err_out) {
+    using CS = ColStream<T, N>;
+    using L = StreamLaunch<T, N>;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev >= kMaxDevices || !g_err_addr[dev] ||
+        L::per_sm[STAGE] < 1 || L::nsm < 1)
+        return false;
+    const int slots = L::nsm * L::per_sm[STAGE];
+    const int grid = a.kc < slots ? a.kc : slots;
+    k_col_stream<T, N, STAGE><<<grid, CS::THREADS, CS::SMEM, a.st>>>(
+        map, (Pair<T>*)a.X, a.kc, (cplx<T>*)a.u0t, (cplx<T>*)a.acct, (const T*)a.tab,
+        (const StepParams<T>*)a.P, (const cplx<T>*)a.tw, g_err_addr[dev]);
+    *err_out = cudaGetLastError();
+    return true;
+}
+
 template <typename T, int N, int STAGE, int BX>
 cudaError_t col_stage(const ColArgs& a) {
     if constexpr (!tile_ok(N, BX)) {
         return cudaErrorInvalidValue;
     } else {
+        if constexpr (BX == 1 && STAGE >= 0 && stream_ok<T, N>()) {
+            CUtensorMap map;
+            cudaError_t e = cudaSuccess;
+            if (a.members == 1 && g_streaming.load(std::memory_order_relaxed) &&
+                x_map<T, N>(&map, a.X, a.kc) && col_stream<T, N, STAGE>(a, map, &e))
+                return e;
+        }
         using F = Fused2D<N, BX>;
         const int grid = (a.kc + F::B - 1) / F::B;
         k_col_pass<T, N, STAGE, BX><<<dim3(grid, a.members), F::THREADS,
@@ -222,6 +343,19 @@ void fill_twiddles(int n, double* out) {
 }
 
 bool tile_supported(int n, int tile) { return tile_ok(n, tile); }
+
+void set_streaming(bool on) { g_streaming.store(on, std::memory_order_relaxed); }
+bool streaming() { return g_streaming.load(std::memory_order_relaxed); }
+
+cudaError_t take_stream_error(unsigned* bits) {
+    unsigned h = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&h, g_stream_err, sizeof(h));
+    if (e) return e;
+    *bits = h;
+    const unsigned zero = 0;
+    if (h) return cudaMemcpyToSymbol(g_stream_err, &zero, sizeof(zero));
+    return cudaSuccess;
+}
 
 bool supported(int n, int fp64) {
     if (n < 16 || (n & (n - 1))) return false;

@@ -24,6 +24,7 @@
 #include "common.cuh"
 #include "fft_block.cuh"
 #include "reduce.cuh"
+#include "tma.cuh"
 
 namespace sp {
 
@@ -209,44 +210,16 @@ __device__ __forceinline__ Pair<T> next_inputs(T kx, T ky, T k2, bool keep, cplx
     return o;
 }
 
-// STAGE 0..3: Lawson stage; STAGE = -1: set-up (no forward transform, no update: the inputs of
-// stage 0 from the state u0t).
-template <typename T, int N, int STAGE, int BX = 1>
-__global__ void __launch_bounds__(Fused2D<N, BX>::THREADS) k_col_pass(
-    Pair<T>* __restrict__ X, int kc, cplx<T>* __restrict__ u0t, cplx<T>* __restrict__ acct,
-    const T* __restrict__ tab, const StepParams<T>* __restrict__ P,
-    const cplx<T>* __restrict__ tw, size_t x_stride, size_t u_stride, int tab_stride) {
-    using F = Fused2D<N, BX>;
-    constexpr int TT = F::T;
-    constexpr int RF0 = first_radix<N, false>();  // forward input pattern
-    constexpr int RL = last_radix<N, false>();    // forward output = inverse input pattern
-    constexpr int RIL = last_radix<N, true>();    // inverse output pattern
-    static_assert(first_radix<N, true>() == RL, "register hand-off");
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int sub = threadIdx.x / TT, t = threadIdx.x % TT;
-    Pair<T>* sm = reinterpret_cast<Pair<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
-    const int ky = blockIdx.x * F::B + sub;
-    const bool active = ky < kc;  // inactive sub-blocks still take part in every barrier
-    X += blockIdx.y * x_stride;
-    u0t += blockIdx.y * u_stride;
-    acct += blockIdx.y * u_stride;
-    tab += blockIdx.y * tab_stride;
-    const StepParams<T> p = P[blockIdx.y];
+// The pointwise middle of a column pass, on the forward transform's output held in registers:
+// v[g*RL + m] belongs to row index i = in_pos<N, RL>(t, g, m).  Nonlinear term, Lawson stage
+// update of u0t / acct, and the next inverse-transform inputs written back into v.
+template <typename T, int N, int STAGE>
+__device__ __forceinline__ void col_update(Pair<T> (&v)[16], int t, int ky, bool active,
+                                           cplx<T>* __restrict__ u0t, cplx<T>* __restrict__ acct,
+                                           const T* __restrict__ tab, const StepParams<T>& p) {
+    constexpr int RL = last_radix<N, false>();
     const T kyr = (T)ky;
     const int nh = N / 2 + 1;
-
-    Pair<T> v[16];
-    if constexpr (STAGE >= 0) {
-#pragma unroll
-        for (int g = 0; g < 16 / RF0; ++g)
-#pragma unroll
-            for (int m = 0; m < RF0; ++m) {
-                const int x = in_pos<N, RF0>(t, g, m);
-                v[g * RF0 + m] = active ? X[xidx(x, ky, kc)] : Pair<T>{mk<T>(0, 0), mk<T>(0, 0)};
-            }
-        block_fft<N, false>(v, sm, t, tw);
-    }
-    // v[g*RL + m] now belongs to row index i = in_pos<N, RL>(t, g, m)
 #pragma unroll
     for (int g = 0; g < 16 / RL; ++g)
 #pragma unroll
@@ -274,6 +247,43 @@ __global__ void __launch_bounds__(Fused2D<N, BX>::THREADS) k_col_pass(
             }
             v[g * RL + m] = next_inputs<T>(kx, kyr, k2, keep, nxt, p.scale);
         }
+}
+
+// STAGE 0..3: Lawson stage; STAGE = -1: set-up (no forward transform, no update: the inputs of
+// stage 0 from the state u0t).
+template <typename T, int N, int STAGE, int BX = 1>
+__global__ void __launch_bounds__(Fused2D<N, BX>::THREADS) k_col_pass(
+    Pair<T>* __restrict__ X, int kc, cplx<T>* __restrict__ u0t, cplx<T>* __restrict__ acct,
+    const T* __restrict__ tab, const StepParams<T>* __restrict__ P,
+    const cplx<T>* __restrict__ tw, size_t x_stride, size_t u_stride, int tab_stride) {
+    using F = Fused2D<N, BX>;
+    constexpr int TT = F::T;
+    constexpr int RF0 = first_radix<N, false>();  // forward input pattern
+    constexpr int RIL = last_radix<N, true>();    // inverse output pattern
+    static_assert(first_radix<N, true>() == last_radix<N, false>(), "register hand-off");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int sub = threadIdx.x / TT, t = threadIdx.x % TT;
+    Pair<T>* sm = reinterpret_cast<Pair<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
+    const int ky = blockIdx.x * F::B + sub;
+    const bool active = ky < kc;  // inactive sub-blocks still take part in every barrier
+    X += blockIdx.y * x_stride;
+    u0t += blockIdx.y * u_stride;
+    acct += blockIdx.y * u_stride;
+    tab += blockIdx.y * tab_stride;
+    const StepParams<T> p = P[blockIdx.y];
+
+    Pair<T> v[16];
+    if constexpr (STAGE >= 0) {
+#pragma unroll
+        for (int g = 0; g < 16 / RF0; ++g)
+#pragma unroll
+            for (int m = 0; m < RF0; ++m) {
+                const int x = in_pos<N, RF0>(t, g, m);
+                v[g * RF0 + m] = active ? X[xidx(x, ky, kc)] : Pair<T>{mk<T>(0, 0), mk<T>(0, 0)};
+            }
+        block_fft<N, false>(v, sm, t, tw);
+    }
+    col_update<T, N, STAGE>(v, t, ky, active, u0t, acct, tab, p);
     __syncthreads();
     block_fft<N, true>(v, sm, t, tw);
     if (active) {
@@ -284,6 +294,107 @@ __global__ void __launch_bounds__(Fused2D<N, BX>::THREADS) k_col_pass(
                 const int x = in_pos<N, RIL>(t, g, m);
                 X[xidx(x, ky, kc)] = v[g * RIL + m];
             }
+    }
+}
+
+// ------------------------------------------------------------------------------- streamed column pass
+// Persistent form of k_col_pass for one run (stages 0..3): CTA b takes columns b, b + grid, ...
+// While a column is transformed in registers, the next column's X data (n Pairs at a stride of
+// one row pair) is already on its way into shared memory by TMA (boxes of 2 Pairs x up to 256
+// row pairs), and the next column's state / accumulator rows are prefetched into L2, so the
+// column's loads no longer wait on HBM.  The two transforms exchange through a buffer of single
+// complex values (exchange_halves), which leaves room for the prefetch buffer.  The tensor map
+// views X as float32 words: row pair q is row q of width kc * 2 * sizeof(Pair) / 4; column ky
+// is the box column at x = ky * stream_box_w<T>().
+template <typename T>
+constexpr int stream_box_w() { return 2 * (int)sizeof(Pair<T>) / 4; }  // words per row pair
+template <int N>
+constexpr int stream_box_h() { return N / 2 < 256 ? N / 2 : 256; }     // row pairs per box
+
+template <typename T, int N>
+struct ColStream {
+    static constexpr int THREADS = N / 16;
+    static constexpr size_t PB_BYTES = (size_t)N * sizeof(Pair<T>);
+    static constexpr size_t EX_BYTES = (size_t)FftPlan<N>::SMEM * sizeof(cplx<T>);
+    static constexpr size_t SMEM = PB_BYTES + EX_BYTES + 16;  // + the mbarrier
+    // CTAs per SM that shared memory (228 KB, 1 KB reserved per CTA) and 128 registers per
+    // thread allow: 1 at n = 8192 fp32, 2 at 4096, 4 at 2048
+    static constexpr int by_smem = (int)(233472 / (SMEM + 1024));
+    static constexpr int by_regs = 65536 / (THREADS * 128);
+    static constexpr int MIN_BLOCKS = by_smem < 1 ? 1 : (by_smem < by_regs ? by_smem : by_regs);
+};
+
+constexpr uint32_t kStreamWait = 1u << 22;  // mbarrier polls before a wait gives up
+
+// Error bit set by a streamed column pass whose TMA data never arrived (the pass then returns).
+constexpr unsigned kStreamTimeout = 1u;
+
+template <typename T, int N, int STAGE>
+__global__ void __launch_bounds__(ColStream<T, N>::THREADS, ColStream<T, N>::MIN_BLOCKS)
+k_col_stream(const __grid_constant__ CUtensorMap xmap, Pair<T>* __restrict__ X, int kc,
+             cplx<T>* __restrict__ u0t, cplx<T>* __restrict__ acct, const T* __restrict__ tab,
+             const StepParams<T>* __restrict__ P, const cplx<T>* __restrict__ tw,
+             unsigned* __restrict__ err) {
+    static_assert(STAGE >= 0, "the set-up pass reads no X");
+    using CS = ColStream<T, N>;
+    constexpr int RF0 = first_radix<N, false>();
+    constexpr int RIL = last_radix<N, true>();
+    constexpr int BW = stream_box_w<T>(), BH = stream_box_h<N>();
+    constexpr int NBOX = (N / 2) / BH;
+    static_assert(first_radix<N, true>() == last_radix<N, false>(), "register hand-off");
+    extern __shared__ __align__(128) unsigned char stream_smem[];
+    Pair<T>* pb = reinterpret_cast<Pair<T>*>(stream_smem);
+    cplx<T>* ex = reinterpret_cast<cplx<T>*>(stream_smem + CS::PB_BYTES);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(stream_smem + CS::PB_BYTES + CS::EX_BYTES);
+    const int t = threadIdx.x;
+    const StepParams<T> p = *P;
+
+    // thread 0: ask for column c's X data (completing on `bar`) and its state rows in L2
+    auto fetch = [&](int c) {
+        tma::arrive_expect_tx(bar, (uint32_t)CS::PB_BYTES);
+#pragma unroll 1
+        for (int b = 0; b < NBOX; ++b)
+            tma::load_2d(pb + (size_t)b * BH * 2, &xmap, c * BW, b * BH, bar);
+        tma::prefetch_l2(u0t + (size_t)c * N, (uint32_t)(N * sizeof(cplx<T>)));
+        if (STAGE > 0) tma::prefetch_l2(acct + (size_t)c * N, (uint32_t)(N * sizeof(cplx<T>)));
+    };
+
+    int ky = blockIdx.x;
+    if (t == 0) {
+        tc::mbar_init(bar, 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+    if (t == 0 && ky < kc) fetch(ky);
+    uint32_t phase = 0;
+    for (; ky < kc; ky += gridDim.x) {
+        const bool ok = tc::mbar_wait(bar, phase, kStreamWait);
+        if (!__syncthreads_and(ok)) {
+            // the copy never completed: report, give it one more bounded wait, leave
+            if (t == 0) {
+                atomicOr(err, kStreamTimeout);
+                tc::mbar_wait(bar, phase, kStreamWait);
+            }
+            return;
+        }
+        phase ^= 1u;
+        Pair<T> v[16];
+#pragma unroll
+        for (int g = 0; g < 16 / RF0; ++g)
+#pragma unroll
+            for (int m = 0; m < RF0; ++m) v[g * RF0 + m] = pb[in_pos<N, RF0>(t, g, m)];
+        __syncthreads();  // every thread has its column: the buffer may be refilled
+        if (t == 0 && ky + (int)gridDim.x < kc) {
+            tc::fence_smem_to_async();
+            fetch(ky + gridDim.x);
+        }
+        block_fft_halves<N, false>(v, ex, t, tw);
+        col_update<T, N, STAGE>(v, t, ky, true, u0t, acct, tab, p);
+        block_fft_halves<N, true>(v, ex, t, tw);
+#pragma unroll
+        for (int g = 0; g < 16 / RIL; ++g)
+#pragma unroll
+            for (int m = 0; m < RIL; ++m) X[xidx(in_pos<N, RIL>(t, g, m), ky, kc)] = v[g * RIL + m];
     }
 }
 

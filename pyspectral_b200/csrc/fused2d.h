@@ -24,6 +24,13 @@ void fill_twiddles(int n, double* out);
 // tile: sub-block multiplier of the row and column passes (1; 2 and 4 for n <= 1024), the
 // ensemble autotuner's choice.
 bool tile_supported(int n, int tile);
+// Process-wide choice of the streamed (persistent, TMA-prefetched) column pass for single runs
+// of n = 2048..8192 (fp64 up to 4096); on by default.  Off: the one-column-per-CTA pass.
+void set_streaming(bool on);
+bool streaming();
+// Error bits the streamed pass raised on this device since the last call (then cleared);
+// synchronous.
+cudaError_t take_stream_error(unsigned* bits);
 cudaError_t row_pass(int n, int fp64, void* X, int kc, const void* tw, cudaStream_t st,
                      int members = 1, size_t x_stride = 0, int tile = 1);
 cudaError_t row_max(int n, int fp64, const void* X, int kc, const void* tw,

@@ -863,6 +863,22 @@ int sp_sync_state(sp_solver* s, void* stream) {
     return SP_OK;
 }
 
+int sp_set_column_streaming(int enable) {
+    sp::fused::set_streaming(enable != 0);
+    return SP_OK;
+}
+int sp_column_streaming(void) { return sp::fused::streaming() ? 1 : 0; }
+
+int sp_take_device_error(unsigned int* bits) {
+    if (!bits) return SP_ERR_ARG;
+    cudaError_t e = sp::fused::take_stream_error(bits);
+    if (e != cudaSuccess) {
+        set_thread_error(cudaGetErrorString(e));
+        return SP_ERR_CUDA;
+    }
+    return SP_OK;
+}
+
 int sp_set_graph(sp_solver* s, int enable) {
     if (!s) return SP_ERR_ARG;
     s->graph_on = enable != 0;

@@ -161,6 +161,7 @@ class B200Solver(SpectralSolver):
         stage = self._host_staging()
         stage.copy_(self.state_native(), non_blocking=True)
         self.torch.cuda.current_stream(self.device).synchronize()
+        _lib.check_device_errors(self.lib)
         return stage.numpy().astype(np.complex128)
 
     def state_native(self) -> Any:
@@ -238,3 +239,13 @@ class B200FusedSolver(B200Solver):
     dims = (2,)
     forms = ("basdevant",)
     fft_mode = _lib.FFT_FUSED
+
+
+def set_column_streaming(enable: bool) -> bool:
+    """Choose the fused 2D engine's column pass for single runs of n = 2048..8192, process-wide
+    (``sp_set_column_streaming``): True = the streamed persistent pass (default), False = one
+    column per CTA.  Graphs captured earlier keep their pass.  Returns the previous setting."""
+    lib = _lib.load()
+    prev = bool(lib.sp_column_streaming())
+    lib.sp_set_column_streaming(int(bool(enable)))
+    return prev

@@ -419,3 +419,39 @@ def test_cli_run_on_device(tmp_path, capsys):
     assert main(["run", "--backend", FUSED, "--n", "64", "--t-end", "0.1", "--case", "tgv",
                  "--dtype", "float64", "--out", str(out)]) == 0
     assert "steps" in capsys.readouterr().out and out.exists()
+
+
+@pytest.mark.parametrize("n,dtype", [(2048, "float32"), (2048, "float64"), (4096, "float32"),
+                                     (4096, "float64"), (8192, "float32")])
+def test_streamed_column_pass_matches_one_column_per_cta(n, dtype):
+    """The persistent TMA-prefetched column pass against the one-column-per-CTA pass (same
+    arithmetic, exchanges in halves; separately compiled, so equal to round-off), plain launches
+    and graph replay, with forcing, drag and a dt change; all runs start from the same state."""
+    from pyspectral_b200 import _lib
+    from pyspectral_b200.solver import set_column_streaming
+
+    cfg = Config(n=n, dim=2, nu=1e-4, alpha=0.1, alpha_kmax=2.0, force_amp=0.2, force_klo=4,
+                 force_khi=6, dtype=dtype)
+    ic = initial.random_phase_2d(n, k0=12, seed=5)
+    out = {}
+    dt = None
+    prev = set_column_streaming(True)
+    try:
+        for on in (True, False):
+            set_column_streaming(on)
+            for graph in (True, False):
+                s = get(FUSED).make(cfg)
+                s._check(s.lib.sp_set_graph(s._h, int(graph)), "sp_set_graph")
+                s.set_state(ic)
+                if dt is None:  # CFL 0.4, so round-off differences are not amplified
+                    dt = 0.4 * (2 * math.pi / n) / s.diag.max_velocity_sum(s.state_native())
+                s.advance(2, dt)
+                s.advance(1, 0.7 * dt)
+                out[(on, graph)] = s.get_state()
+    finally:
+        set_column_streaming(prev)
+    _lib.check_device_errors(_lib.load())
+    tol = 1e-13 if dtype == "float64" else 2e-6  # fp32: round-off of two instantiations
+    ref = out[(False, True)]
+    for key, a in out.items():
+        assert rel(a, ref) < tol, key
