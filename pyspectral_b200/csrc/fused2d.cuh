@@ -303,7 +303,10 @@ __global__ void __launch_bounds__(Fused2D<N, BX>::THREADS) k_col_pass(
 // one row pair) is already on its way into shared memory by TMA (boxes of 2 Pairs x up to 256
 // row pairs), and the next column's state / accumulator rows are prefetched into L2, so the
 // column's loads no longer wait on HBM.  The two transforms exchange through a buffer of single
-// complex values (exchange_halves), which leaves room for the prefetch buffer.  The tensor map
+// complex values (exchange_halves), which leaves room for the prefetch buffer.  (Exchanging
+// whole Pairs through the prefetch buffer in the forward transform and starting the next copy
+// after it saves half the barriers but leaves the copy too little time: slower at n = 8192.)
+// The tensor map
 // views X as float32 words: row pair q is row q of width kc * 2 * sizeof(Pair) / 4; column ky
 // is the box column at x = ky * stream_box_w<T>().
 template <typename T>
@@ -349,14 +352,22 @@ k_col_stream(const __grid_constant__ CUtensorMap xmap, Pair<T>* __restrict__ X, 
     const int t = threadIdx.x;
     const StepParams<T> p = *P;
 
-    // thread 0: ask for column c's X data (completing on `bar`) and its state rows in L2
+    // kept rows of a state column: i < LO and i >= HI (|kx| < n/3), rounded out to 16 bytes
+    constexpr int EPB = 16 / (int)sizeof(cplx<T>);  // elements per 16 bytes
+    constexpr int LO = (((N - 1) / 3 + 1) + EPB - 1) / EPB * EPB;
+    constexpr int HI = (N - (N - 1) / 3) / EPB * EPB;
+    // thread 0: ask for column c's X data (completing on `bar`) and its kept state rows in L2
     auto fetch = [&](int c) {
         tma::arrive_expect_tx(bar, (uint32_t)CS::PB_BYTES);
 #pragma unroll 1
         for (int b = 0; b < NBOX; ++b)
             tma::load_2d(pb + (size_t)b * BH * 2, &xmap, c * BW, b * BH, bar);
-        tma::prefetch_l2(u0t + (size_t)c * N, (uint32_t)(N * sizeof(cplx<T>)));
-        if (STAGE > 0) tma::prefetch_l2(acct + (size_t)c * N, (uint32_t)(N * sizeof(cplx<T>)));
+        tma::prefetch_l2(u0t + (size_t)c * N, (uint32_t)(LO * sizeof(cplx<T>)));
+        tma::prefetch_l2(u0t + (size_t)c * N + HI, (uint32_t)((N - HI) * sizeof(cplx<T>)));
+        if (STAGE > 0) {
+            tma::prefetch_l2(acct + (size_t)c * N, (uint32_t)(LO * sizeof(cplx<T>)));
+            tma::prefetch_l2(acct + (size_t)c * N + HI, (uint32_t)((N - HI) * sizeof(cplx<T>)));
+        }
     };
 
     int ky = blockIdx.x;
