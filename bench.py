@@ -687,7 +687,11 @@ def ours(args, w: dict) -> int:
         t_col = event_time_ms(lambda: s.run_phase(3, 1), 15)
         row_bytes = 2 * n * kc * 2 * sc          # read + write the (n x kc) pair array
         col_bytes = 2 * n * kc * 2 * sc + 3 * kept_rows * kc * sc  # + state, acc r/w
-        kernels = {"k_row_pass": (t_row, row_bytes), "k_col_pass<stage 1>": (t_col, col_bytes)}
+        # the streamed persistent column pass runs single runs of n = 2048..8192 (fp64 <= 4096)
+        streamed = (bool(s.lib.sp_column_streaming()) and 2048 <= n
+                    and n <= (4096 if w["dtype"] == "float64" else 8192))
+        cname = "k_col_stream<stage 1>" if streamed else "k_col_pass<stage 1>"
+        kernels = {"k_row_pass": (t_row, row_bytes), cname: (t_col, col_bytes)}
         del cf
     else:
         t_phys = event_time_ms(lambda: s.run_phase(1), 15)
