@@ -145,3 +145,15 @@ def test_study_config_cutoffs():
     assert sc.batch_tiles * 128 == 65536 and sc.train_steps == 20000
     small = StudyConfig.small()
     assert small.k_check == 42 and 3 * small.k_check < small.n_coarse <= 3 * (small.k_check + 1)
+
+
+def test_cutoff_ramp_rises_from_the_ramp_start_to_the_cutoff():
+    from pyspectral_b200.closure_les import StudyConfig, cutoff_ramp
+
+    sc = StudyConfig()
+    r = cutoff_ramp(sc, 182)
+    kc, k0 = sc.k_check, sc.cutoff_from * sc.k_check
+    assert r.dtype == np.float32 and r.shape == (182,)
+    assert np.all(r[: int(k0) + 1] == 0)
+    assert abs(r[kc] - 1.0) < 1e-6
+    assert np.all(np.diff(r) >= 0) and abs(r.max() - 2.25) < 1e-6
