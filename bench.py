@@ -25,6 +25,7 @@ pyspectral's NumpySolver) on the same workload instead, on rank 0 only.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import math
 import os
@@ -54,6 +55,9 @@ WORKLOADS = {
                                       form="rotational", ic="tgv3d", cfl=0.5),
     "tgv3d-512-fp32-basdevant": dict(n=512, dim=3, dtype="float32", nu=1 / 1600,
                                      form="basdevant", ic="tgv3d", cfl=0.5),
+    # the same flow on 1024^3 with the lean-memory engine (per-field plans), a few steps
+    "tgv3d-1024-fp32-lean": dict(n=1024, dim=3, dtype="float32", nu=1 / 1600,
+                                 form="rotational", ic="tgv3d", cfl=0.5, big=True),
     # 256 forced runs of uneven size advanced together: 64 each at 128^2 .. 1024^2, fp32
     "ensemble-4x64-fp32": dict(ensemble=True, sizes=(128, 256, 512, 1024), per_size=64,
                                dtype="float32", dim=2, form="basdevant", k0=8.0, power=1e-3,
@@ -241,6 +245,149 @@ def copy_bandwidth_gbs(nbytes: int = 1 << 30) -> float:
     del a, b
     torch.cuda.empty_cache()
     return 2 * nbytes / (best * 1e-3) / 1e9
+
+
+def tgv3d_device(n: int, dtype) -> "torch.Tensor":  # noqa: F821
+    """The 3D Taylor-Green state built on the device: its only modes are (+-1, +-1, +-1), whose
+    coefficients are those of the 8^3 transform scaled by (n/8)^3 (no n^3 host arrays)."""
+    import torch
+
+    from pyspectral_b200 import initial
+
+    small = initial.to_spectral(initial.taylor_green_3d(8), 3) * (n / 8.0) ** 3
+    out = torch.zeros((3, n, n, n // 2 + 1), dtype=dtype, device="cuda")
+    for i in (1, 7):
+        for j in (1, 7):
+            out[:, i if i == 1 else n - 1, j if j == 1 else n - 1, 1] = torch.from_numpy(
+                small[:, i, j, 1]).to(dtype).to(out.device)
+    return out
+
+
+def ours_big3d(args, w: dict) -> int:
+    """A 3D grid too large for the usual set of solvers side by side (1024^3): one lean solver
+    is timed, then its phases; the e2e pass reuses it (host state in and out) when the host has
+    the memory; the one-step error against the fp64 lean engine is computed on the device with
+    the fp32 solver freed first."""
+    import psutil
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    comm = Replicas("nccl", torch.device("cuda", local))
+    barrier, max_over_ranks = comm.barrier, comm.max
+
+    from pyspectral_b200.registry import make_solver
+
+    variant = "b200/fused-inplace-lean"
+    cfg = make_config(w)
+    n = w["n"]
+    ic = tgv3d_device(n, torch.complex64)
+    s = make_solver(variant, cfg)
+    s.set_state(ic)
+    run_workload(s, w, args.warmup)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = s.kernel_launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    run_workload(s, w, args.steps)
+    ev1.record()
+    ev1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = s.kernel_launches - l0
+    ms_step = max_over_ranks(ev0.elapsed_time(ev1)) / args.steps
+    npts = float(n) ** 3
+    value = aggregate_mpts(world, npts, ms_step * 1e-3)
+
+    # per-phase device times of a middle stage (state garbage afterwards)
+    t_fft = event_time_ms(lambda: (s.run_phase(0), s.run_phase(2)), 5)
+    t_phys = event_time_ms(lambda: s.run_phase(1), 5)
+    t_post = event_time_ms(lambda: s.run_phase(3, 1), 5)
+    tm = traffic_model(n, 3, w["form"], w["dtype"])
+    bcopy = copy_bandwidth_gbs()
+    t_roof_ms = 4 * t_fft + tm["pointwise_bytes"] / (bcopy * 1e9) * 1e3
+    ninv, nfwd, nmodes = s.n_inv, s.n_fwd, tm["modes"]
+    post_bytes = (nfwd + 2 * 3 + 3 + ninv) * nmodes * 8
+    phys_bytes = (ninv + nfwd) * nmodes * 8
+    kernels = {"k_post3d<stage 1>": (t_post, post_bytes), "k_phys": (t_phys, phys_bytes)}
+    kname = max(kernels, key=lambda k: kernels[k][0])
+    k_ms, k_bytes = kernels[kname]
+    hbm = measured_peaks().get("hbm_gbs")
+    achieved = k_bytes / (k_ms * 1e-3) / 1e9
+
+    # end to end through the public API on the same solver, if the host can hold the state
+    state_bytes = s.u0.nbytes
+    e2e = None
+    if psutil.virtual_memory().available > 8 * state_bytes:
+        host_ic = ic.cpu().numpy()
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        s.set_state(host_ic)
+        run_workload(s, w, args.steps)
+        out = s.get_state()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        del out, host_ic
+        e2e = {"value": world * npts * args.steps / e2e_s / 1e6, "unit": "Mpts/s",
+               "h2d_bytes_per_step": state_bytes / args.steps,
+               "d2h_bytes_per_step": state_bytes / args.steps,
+               "what": "set_state(host) + K steps + get_state(host), wall clock"}
+    else:
+        e2e = {"value": None, "unit": "Mpts/s", "h2d_bytes_per_step": state_bytes / args.steps,
+               "d2h_bytes_per_step": state_bytes / args.steps,
+               "what": "skipped: host memory below 8x the state"}
+
+    # one CFL step against the fp64 lean engine, compared on the device
+    s.set_state(ic)
+    h = min(0.05, w["cfl"] * (2 * math.pi / n) / s.diag.max_velocity_sum(s.state_native()))
+    s.step(h)
+    ua = s.state_native().clone()
+    del s
+    ic = None
+    gc.collect()  # the solver's diagnostics refer back to it
+    torch.cuda.empty_cache()
+    b = make_solver(variant, cfg.with_(dtype="float64"))
+    b.set_state(tgv3d_device(n, torch.complex128))
+    b.step(h)
+    ub = b.state_native()
+    num = max(float((ua[c].to(torch.complex128) - ub[c]).abs().max()) for c in range(3))
+    rel_err = num / float(ub.abs().max())
+    del b, ua, ub
+    gc.collect()
+    torch.cuda.empty_cache()
+
+    line = {
+        "metric": "Mpts/s/RK4 step", "value": value, "unit": "Mpts/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "n": n, "dim": 3, "form": w["form"],
+                   "nu": w["nu"], "variant": variant, "cfl": w["cfl"],
+                   "parallelism": "replicas" if world > 1 else "single", "l2": l2_note(w)},
+        "pct_fft_roofline": 100.0 * t_roof_ms / ms_step,
+        "fft_roofline": {"t_fft_stage_ms": t_fft, "t_fft_stage_ms_own_plans": t_fft,
+                         "t_fft_stage_ms_torch_fft": None,
+                         "note": "own per-field plans only (torch.fft at 1024^3 not run)",
+                         "t_roofline_step_ms": t_roof_ms, "copy_bw_gbs": bcopy,
+                         "pointwise_bytes": tm["pointwise_bytes"],
+                         "model_bytes_per_step": tm["total_bytes"],
+                         "own_kernels_ms": {k: v[0] for k, v in kernels.items()}},
+        "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
+                     "peak": hbm or FALLBACK_HBM_GBS, "unit": "GB/s",
+                     "frac": achieved / (hbm or FALLBACK_HBM_GBS),
+                     "peak_source": "measured" if hbm else "fallback",
+                     "algorithmic_bytes_per_launch": k_bytes, "traffic": None},
+        "e2e": e2e, "rel_err_one_step_vs_fp64": rel_err, "gpu_launches": launches,
+        "clocks": clk,
+        "memory_gb": {"fp32_solver": 12 * state_bytes / 3 / 1e9},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    comm.close()
+    return 0
 
 
 def run_workload(s, w: dict, nsteps: int) -> None:
@@ -808,6 +955,16 @@ def main(argv: list[str] | None = None) -> int:
                         "d2h_bytes_per_step": 0}}), flush=True)
             return 0
         return ours_ensemble(args, w)
+    if w.get("big"):
+        if args.impl == "reference":
+            rank, _, _ = dist_env()
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "a 1024^3 step of the NumPy oracle needs about 100 GB of host "
+                                  "memory and minutes per step; the 512^3 workloads carry the "
+                                  "CPU baseline"}))
+            return 0
+        return ours_big3d(args, w)
     if args.variant == "auto":
         n = w["n"]
         fused_ok = (w["dim"] == 2 and n & (n - 1) == 0 and 16 <= n

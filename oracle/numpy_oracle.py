@@ -277,3 +277,44 @@ def run_fixed(solver: Any, nsteps: int, dt: float) -> np.ndarray:
     """Advance and return the state (convenience for tests)."""
     solver.advance(nsteps, dt)
     return solver.get_state()
+
+
+def cfl_dt(solver: OracleSolver, diag: OracleDiagnostics, cfl: float, dt_max: float) -> float:
+    """simulate.py:31-37: cfl * dx / sum_i max|u_i|, capped at dt_max (dt_max if the bound is
+    0 or not finite)."""
+    umax = diag.max_velocity_sum(solver.state)
+    if not (umax > 0.0) or not np.isfinite(umax):
+        return dt_max
+    return min(dt_max, cfl * (2.0 * np.pi / solver.n) / umax)
+
+
+def run_cfl(solver: OracleSolver, t_end: float, *, cfl: float = 0.5, dt_max: float = 0.05,
+            cfl_every: int = 10, diag_dt: float | None = None) -> dict[str, Any]:
+    """simulate.py:40-96 without forcing control or callbacks: CFL-adaptive steps (dt
+    refreshed every cfl_every steps), the step clipped to the next record time and to t_end;
+    energy and enstrophy recorded at t = 0, every diag_dt and at t_end."""
+    diag = OracleDiagnostics(solver.n, solver.dim)
+    out: dict[str, Any] = {"t": [], "energy": [], "enstrophy": [], "steps": 0}
+
+    def record() -> None:
+        out["t"].append(solver.t)
+        out["energy"].append(diag.energy(solver.state))
+        out["enstrophy"].append(diag.enstrophy(solver.state))
+
+    record()
+    tol = 1e-12 * max(1.0, t_end)
+    next_diag = solver.t + diag_dt if diag_dt else np.inf
+    h_cfl = cfl_dt(solver, diag, cfl, dt_max)
+    k = 0
+    while solver.t < t_end - tol:
+        if k % cfl_every == 0 and k > 0:
+            h_cfl = cfl_dt(solver, diag, cfl, dt_max)
+        solver.step(min(h_cfl, t_end - solver.t, next_diag - solver.t))
+        k += 1
+        if solver.t >= next_diag - tol:
+            record()
+            next_diag += diag_dt  # type: ignore[operator]
+    if out["t"][-1] < solver.t - tol:
+        record()
+    out["steps"] = k
+    return out

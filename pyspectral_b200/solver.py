@@ -127,7 +127,8 @@ class B200Solver(SpectralSolver):
 
         Same contract as check_state + set_state of the reference (shape ValueError, 2/3 mask),
         with the mask applied on the device by the engine's load kernel: the host only casts
-        into a pinned staging buffer, the copy to the device is asynchronous.
+        into a pinned staging buffer (torch's threaded copy), the copy to the device is
+        asynchronous.
         """
         torch = self.torch
         if isinstance(state_hat, torch.Tensor) and state_hat.is_cuda:
@@ -141,7 +142,10 @@ class B200Solver(SpectralSolver):
             if a.shape != self.state_shape():
                 raise ValueError(f"state shape {a.shape} != {self.state_shape()}")
             stage = self._host_staging()
-            np.copyto(stage.numpy(), a, casting="unsafe")
+            # torch's CPU copy casts with all host threads (numpy's copyto casts on one)
+            if a.dtype not in (np.complex64, np.complex128, np.float32, np.float64):
+                a = a.astype(np.complex128)
+            stage.copy_(torch.from_numpy(np.ascontiguousarray(a)))
             self.u0.copy_(stage, non_blocking=True)
             self._staging_free.record(torch.cuda.current_stream(self.device))
         self._check(self.lib.sp_prepare(self._h, self._stream()), "sp_prepare")
@@ -157,12 +161,16 @@ class B200Solver(SpectralSolver):
         return self._staging
 
     def get_state(self) -> np.ndarray:
-        """The state copied to the host as complex128 (through the pinned staging buffer)."""
+        """The state copied to the host as complex128 (through the pinned staging buffer; the
+        widening cast runs on all host threads)."""
+        torch = self.torch
         stage = self._host_staging()
         stage.copy_(self.state_native(), non_blocking=True)
-        self.torch.cuda.current_stream(self.device).synchronize()
+        torch.cuda.current_stream(self.device).synchronize()
         _lib.check_device_errors(self.lib)
-        return stage.numpy().astype(np.complex128)
+        out = torch.empty(stage.shape, dtype=torch.complex128)
+        out.copy_(stage)
+        return out.numpy()
 
     def state_native(self) -> Any:
         """The live state (NumPy r2c layout).  Engines that advance a transposed copy write it
