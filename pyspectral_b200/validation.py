@@ -1,4 +1,5 @@
-"""Physics validation runs on the device: the 3D Taylor-Green vortex at Re = 1600.
+"""Physics validation runs on the device: the 3D Taylor-Green vortex at Re = 1600 and the
+IF-RK4 temporal order.
 
 Mirrors ``pyspectral.validation.tgv3d`` (src/pyspectral/validation.py:152-200): the run from
 u = sin x cos y cos z, v = -cos x sin y cos z, w = 0 with nu = 1/1600 to t_end under
@@ -62,6 +63,27 @@ def compare_dissipation(t: np.ndarray, eps: np.ndarray, reference: dict[str, Any
         "ref_peak_value": peak, "ref_peak_time": float(tr[int(np.argmax(er))]),
         "peak_rel_err": float((eps[i] - peak) / peak),
     }
+
+
+def temporal_convergence(variant: str = "b200/fused-inplace-graph",
+                         dts: tuple[float, ...] = (0.04, 0.02, 0.01, 0.005, 0.0025), n: int = 64,
+                         nu: float = 0.01, t_end: float = 1.0) -> dict[str, Any]:
+    """IF-RK4 self-convergence on a nonlinear 2D flow, fp64 (validation.py:86-100): errors of
+    each dt against a run at min(dts)/8 and the least-squares order (slope of log err vs log
+    dt; the reference's NumPy path measures 3.99)."""
+    w0 = initial.to_spectral(initial.smooth_2d(n), 2)
+
+    def solve(dt: float) -> np.ndarray:
+        s = make_solver(variant, Config(n=n, dim=2, nu=nu, dtype="float64"))
+        s.set_state(w0)
+        s.advance(int(round(t_end / dt)), dt)
+        return s.get_state()
+
+    ref = solve(min(dts) / 8)
+    errs = [float(np.abs(solve(dt) - ref).max() / np.abs(ref).max()) for dt in dts]
+    order = float(np.polyfit(np.log(np.array(dts)), np.log(np.array(errs)), 1)[0])
+    return {"variant": variant, "dt": list(dts), "err": errs, "order": order, "n": n, "nu": nu,
+            "t_end": t_end}
 
 
 def main(argv: list[str] | None = None) -> int:

@@ -1,4 +1,5 @@
-"""3D Taylor-Green vortex at Re = 1600 to t = 10 against the fp64 oracle's run at 128^3.
+"""3D Taylor-Green vortex at Re = 1600 to t = 10 against the fp64 oracle's run at 128^3, and the
+IF-RK4 temporal order on the device.
 
 The reference validates this flow by its dissipation eps(t) = 2 nu Z(t)
 (src/pyspectral/validation.py:152-200).  tests/golden/tgv3d_re1600_n128_fp64.json is the
@@ -42,3 +43,13 @@ def test_tgv3d_128_fp32_dissipation_follows_the_oracle():
     c = compare_dissipation(np.array(r["t"]), np.array(r["dissipation_2nuZ"]), REF)
     assert c["max_abs_err_over_peak"] < 1e-3
     assert abs(c["peak_rel_err"]) < 1e-3
+
+
+@pytest.mark.parametrize("variant", ["b200/fused-inplace-graph", "b200/fused-fft-graph"])
+def test_ifrk4_self_convergence_is_fourth_order_on_the_device(variant):
+    """validation.py:86-100 on the device engines (fp64, 64^2 nonlinear flow): order ~ 4."""
+    from pyspectral_b200.validation import temporal_convergence
+
+    r = temporal_convergence(variant)
+    assert 3.8 < r["order"] < 4.3, r
+    assert r["err"][-1] < 1e-8
