@@ -148,6 +148,13 @@ int sp_column_streaming(void);
  * counterpart. */
 int sp_take_device_error(unsigned int* bits);
 
+/* Failure-path check without a fault: launches one block whose mbarrier wait for a copy that is
+ * never issued gives up after `polls` polls (1..2^20; a poll suspends for at most a few
+ * microseconds), exactly as the streamed passes' waits do, and sets bit 1 of the device error
+ * word (read and cleared by sp_take_device_error).  Nothing stays in flight; the context stays
+ * usable.  No reference counterpart. */
+int sp_wait_probe(unsigned int polls, void* stream);
+
 /* Spectral reductions of a state array (device pointer in the u0 layout, e.g. u0 itself):
  * writes SP_DIAG_COUNT doubles to out (host) — energy, enstrophy, palinstrophy and the energy in
  * band_klo <= |k| <= band_khi — summed in fp64 in a fixed order.  Synchronises `stream`. */

@@ -45,6 +45,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_set_column_streaming": (_i, [_i]),
     "sp_column_streaming": (_i, []),
     "sp_take_device_error": (_i, [ctypes.POINTER(ctypes.c_uint)]),
+    "sp_wait_probe": (_i, [ctypes.c_uint, _vp]),
     "sp_diagnostics": (_i, [_vp, _vp, _d, _d, _dp, _vp]),
     "sp_max_velocity": (_i, [_vp, _vp, _dp, _dp, _vp]),
     "sp_spectrum": (_i, [_vp, _vp, _dp, _i, _vp]),

@@ -347,6 +347,17 @@ bool tile_supported(int n, int tile) { return tile_ok(n, tile); }
 void set_streaming(bool on) { g_streaming.store(on, std::memory_order_relaxed); }
 bool streaming() { return g_streaming.load(std::memory_order_relaxed); }
 
+cudaError_t wait_probe(unsigned polls, cudaStream_t st) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e) return e;
+    if (dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    if (!g_err_addr[dev] && (e = cudaGetSymbolAddress((void**)&g_err_addr[dev], g_stream_err)))
+        return e;
+    k_wait_probe<<<1, 32, 0, st>>>(g_err_addr[dev], polls);
+    return cudaGetLastError();
+}
+
 cudaError_t take_stream_error(unsigned* bits) {
     unsigned h = 0;
     cudaError_t e = cudaMemcpyFromSymbol(&h, g_stream_err, sizeof(h));

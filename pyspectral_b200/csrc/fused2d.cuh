@@ -409,6 +409,21 @@ k_col_stream(const __grid_constant__ CUtensorMap xmap, Pair<T>* __restrict__ X, 
     }
 }
 
+// The time-out path of the streamed passes on its own: one block arms an mbarrier for a copy
+// that is never issued, waits `polls` polls (bounded, as the passes do), records
+// kStreamTimeout and returns.  Nothing is in flight when it exits.
+__global__ void __launch_bounds__(32) k_wait_probe(unsigned* __restrict__ err, uint32_t polls) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar, 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) tma::arrive_expect_tx(&bar, 16);  // 16 bytes that never arrive
+    const bool ok = tc::mbar_wait(&bar, 0, polls);
+    if (!__syncthreads_and(ok) && threadIdx.x == 0) atomicOr(err, kStreamTimeout);
+}
+
 // ------------------------------------------------------------------------------- layout moves
 // u0 (n, nh) NumPy layout -> u0t (kc, n): 32 x 32 tiles through shared memory.
 template <typename T>

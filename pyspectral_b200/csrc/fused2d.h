@@ -31,6 +31,9 @@ bool streaming();
 // Error bits the streamed pass raised on this device since the last call (then cleared);
 // synchronous.
 cudaError_t take_stream_error(unsigned* bits);
+// One block whose bounded mbarrier wait cannot complete: raises the streamed pass's time-out
+// bit after `polls` polls (the failure path, exercised without a fault).
+cudaError_t wait_probe(unsigned polls, cudaStream_t st);
 cudaError_t row_pass(int n, int fp64, void* X, int kc, const void* tw, cudaStream_t st,
                      int members = 1, size_t x_stride = 0, int tile = 1);
 cudaError_t row_max(int n, int fp64, const void* X, int kc, const void* tw,

@@ -879,6 +879,19 @@ int sp_take_device_error(unsigned int* bits) {
     return SP_OK;
 }
 
+int sp_wait_probe(unsigned int polls, void* stream) {
+    if (polls == 0 || polls > (1u << 20)) {
+        set_thread_error("sp_wait_probe: polls must be 1..2^20");
+        return SP_ERR_ARG;
+    }
+    cudaError_t e = sp::fused::wait_probe(polls, (cudaStream_t)stream);
+    if (e != cudaSuccess) {
+        set_thread_error(cudaGetErrorString(e));
+        return SP_ERR_CUDA;
+    }
+    return SP_OK;
+}
+
 int sp_set_graph(sp_solver* s, int enable) {
     if (!s) return SP_ERR_ARG;
     s->graph_on = enable != 0;

@@ -455,3 +455,37 @@ def test_streamed_column_pass_matches_one_column_per_cta(n, dtype):
     ref = out[(False, True)]
     for key, a in out.items():
         assert rel(a, ref) < tol, key
+
+
+def test_bounded_wait_time_out_is_reported_and_the_context_stays_usable():
+    """The streamed passes' mbarrier waits give up after a poll limit and set an error bit
+    instead of hanging.  sp_wait_probe runs that path on a wait nothing completes: the bit is
+    reported once, cleared by the read, and a streamed run afterwards still matches."""
+    import ctypes
+
+    import torch
+
+    from pyspectral_b200 import _lib
+
+    lib = _lib.load()
+    bits = ctypes.c_uint(0)
+    assert lib.sp_take_device_error(ctypes.byref(bits)) == 0  # clear anything earlier
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert lib.sp_wait_probe(0, st) != 0 and lib.sp_wait_probe((1 << 20) + 1, st) != 0
+    assert lib.sp_wait_probe(1000, st) == 0
+    torch.cuda.synchronize()
+    assert lib.sp_take_device_error(ctypes.byref(bits)) == 0 and bits.value == 1
+    assert lib.sp_take_device_error(ctypes.byref(bits)) == 0 and bits.value == 0
+    with pytest.raises(_lib.EngineError):
+        assert lib.sp_wait_probe(10, st) == 0
+        torch.cuda.synchronize()
+        _lib.check_device_errors(lib)
+    cfg = Config(n=2048, dim=2, nu=1e-4, dtype="float32")
+    ic = initial.random_phase_2d(2048, k0=12, seed=2)
+    s = get(FUSED).make(cfg)
+    s.set_state(ic)
+    s.advance(2, 1e-4)
+    ref = _oracle(cfg)
+    ref.set_state(ic)
+    ref.advance(2, 1e-4)
+    assert rel(s.get_state(), ref.get_state()) < TOL["float32"]
