@@ -382,6 +382,35 @@ __device__ __forceinline__ void exchange_halves(Pair<T> (&v)[16], cplx<T>* sm, i
     }
 }
 
+// Twiddled pass of radix 2 at stride S = N/2 (the last inverse pass of N = 2 * 16^k): group g of
+// thread t has js = t + (N/16) g, so w^js = w^t * exp(DIR 2 pi i g / 16): one table load per
+// thread and constant rotations instead of one load per group.
+template <int N, int DIR, typename E, typename C>
+__device__ __forceinline__ void pass_radix2_half(E (&v)[16], int t, const C* __restrict__ tw) {
+    const C w1 = tw_load<DIR>(tw, t);
+    C w[8];
+    w[0] = w1;
+    w[1] = rot16<DIR, 1>(w1);
+    w[2] = rot16<DIR, 2>(w1);
+    w[3] = rot16<DIR, 3>(w1);
+    w[4] = rot16<DIR, 4>(w1);
+    w[5] = rot16<DIR, 5>(w1);
+    w[6] = rot16<DIR, 6>(w1);
+    w[7] = rot16<DIR, 7>(w1);
+#pragma unroll
+    for (int g = 0; g < 8; ++g) {
+        v[g * 2 + 1] = emul(v[g * 2 + 1], w[g]);
+        dft2<DIR>(v + g * 2);
+    }
+}
+
+// pass_compute, with pass_radix2_half for the radix-2 pass at stride N/2.
+template <int N, int R, int S, int DIR, typename E, typename C>
+__device__ __forceinline__ void pass_compute_h(E (&v)[16], int t, const C* __restrict__ tw) {
+    if constexpr (R == 2 && S == N / 2 && N / 16 * 8 == S) pass_radix2_half<N, DIR>(v, t, tw);
+    else pass_compute<N, R, S, DIR>(v, t, tw);
+}
+
 // block_fft of Pair elements with the exchanges of exchange_halves: `sm` holds
 // FftPlan<N>::SMEM complex values instead of Pairs.
 template <int N, bool INV, typename T, typename C>
@@ -394,15 +423,15 @@ __device__ __forceinline__ void block_fft_halves(Pair<T> (&v)[16], cplx<T>* sm, 
     if constexpr (P::NP > 1) {
         constexpr int R1 = P::radix(INV, 1), S1 = P::stride(INV, 1);
         exchange_halves<N, R0, S0, R1>(v, sm, t);
-        pass_compute<N, R1, S1, DIR>(v, t, tw + P::tw_offset(INV, 1));
+        pass_compute_h<N, R1, S1, DIR>(v, t, tw + P::tw_offset(INV, 1));
         if constexpr (P::NP > 2) {
             constexpr int R2 = P::radix(INV, 2), S2 = P::stride(INV, 2);
             exchange_halves<N, R1, S1, R2>(v, sm, t);
-            pass_compute<N, R2, S2, DIR>(v, t, tw + P::tw_offset(INV, 2));
+            pass_compute_h<N, R2, S2, DIR>(v, t, tw + P::tw_offset(INV, 2));
             if constexpr (P::NP > 3) {
                 constexpr int R3 = P::radix(INV, 3), S3 = P::stride(INV, 3);
                 exchange_halves<N, R2, S2, R3>(v, sm, t);
-                pass_compute<N, R3, S3, DIR>(v, t, tw + P::tw_offset(INV, 3));
+                pass_compute_h<N, R3, S3, DIR>(v, t, tw + P::tw_offset(INV, 3));
             }
         }
     }
