@@ -55,6 +55,9 @@ WORKLOADS = {
                                       form="rotational", ic="tgv3d", cfl=0.5),
     "tgv3d-512-fp32-basdevant": dict(n=512, dim=3, dtype="float32", nu=1 / 1600,
                                      form="basdevant", ic="tgv3d", cfl=0.5),
+    # the same flow on 256^3 (profiling captures that must stay small; > 0.7 GB per stage)
+    "tgv3d-256-fp32-basdevant": dict(n=256, dim=3, dtype="float32", nu=1 / 1600,
+                                     form="basdevant", ic="tgv3d", cfl=0.5),
     # the same flow on 1024^3 with the lean-memory engine (per-field plans), a few steps
     "tgv3d-1024-fp32-lean": dict(n=1024, dim=3, dtype="float32", nu=1 / 1600,
                                  form="rotational", ic="tgv3d", cfl=0.5, big=True),
