@@ -204,3 +204,25 @@ def test_sharded_ensemble_on_one_rank_is_the_ensemble():
         b.step(dt)
     np.testing.assert_array_equal(a.diagnostics(3.0, 5.0), b.diagnostics(3.0, 5.0))
     np.testing.assert_array_equal(a.max_velocity_sum(), b.max_velocity_sum())
+
+
+@pytest.mark.parametrize("count", [1, 2])
+def test_large_class_matches_single_runs(count):
+    """A 2048^2 size class: one member runs the streamed persistent column pass (as a single
+    run does), two members the batched one-column-per-CTA pass; both equal single runs (to
+    round-off: separately compiled kernels)."""
+    from pyspectral_b200.ensemble import Ensemble
+
+    cfgs = [Config(n=2048, dim=2, nu=1e-4, alpha=0.1, alpha_kmax=2.0, force_amp=0.2 + 0.1 * i,
+                   force_klo=4, force_khi=6, dtype="float32") for i in range(count)]
+    ics = _ics(cfgs)
+    ens = Ensemble(cfgs, autotune=False)
+    ens.set_states(ics)
+    for _ in range(3):
+        ens.step(np.full(count, 2e-4))
+    for i, c in enumerate(cfgs):
+        s = get(FUSED).make(c)
+        s.set_state(ics[i])
+        s.advance(3, 2e-4)
+        ref = s.get_state()
+        assert np.abs(ens.get_state(i) - ref).max() <= 2e-6 * np.abs(ref).max(), i
