@@ -1,5 +1,5 @@
-"""Physics validation runs on the device: the 3D Taylor-Green vortex at Re = 1600 and the
-IF-RK4 temporal order.
+"""Physics validation runs on the device: the 3D Taylor-Green vortex at Re = 1600, the IF-RK4
+temporal order and the spectral convergence in n.
 
 Mirrors ``pyspectral.validation.tgv3d`` (src/pyspectral/validation.py:152-200): the run from
 u = sin x cos y cos z, v = -cos x sin y cos z, w = 0 with nu = 1/1600 to t_end under
@@ -84,6 +84,41 @@ def temporal_convergence(variant: str = "b200/fused-inplace-graph",
     order = float(np.polyfit(np.log(np.array(dts)), np.log(np.array(errs)), 1)[0])
     return {"variant": variant, "dt": list(dts), "err": errs, "order": order, "n": n, "nu": nu,
             "t_end": t_end}
+
+
+def pad_spectrum(a: np.ndarray, n_to: int) -> np.ndarray:
+    """A 2D r2c spectrum of grid n carried to grid n_to with the same physical amplitudes
+    (validation.py:24-35): modes |kx| < m and 0 <= ky < m, m = min(n, n_to) // 2, copied and
+    scaled by (n_to / n)^2 for the unnormalised transform; every other mode zero."""
+    n = a.shape[-2]
+    m = min(n, n_to) // 2
+    out = np.zeros((n_to, n_to // 2 + 1), dtype=a.dtype)
+    kx = np.r_[0:m, -m + 1:0]
+    out[np.ix_(kx % n_to, np.arange(m))] = a[np.ix_(kx % n, np.arange(m))] * (n_to / n) ** 2
+    return out
+
+
+def spatial_convergence(variant: str = "b200/fused-inplace-graph",
+                        ns: tuple[int, ...] = (8, 12, 16, 20, 24, 32, 40, 48, 64),
+                        n_ref: int = 192, nu: float = 0.02, t_end: float = 0.5,
+                        dt: float = 2.5e-3) -> dict[str, Any]:
+    """Spectral convergence in n of a smooth, non-band-limited 2D flow, fp64
+    (validation.py:103-119): each grid's run to t_end carried to n_ref and compared in physical
+    space with the n_ref run (max error / max value)."""
+
+    def solve(n: int) -> np.ndarray:
+        s = make_solver(variant, Config(n=n, dim=2, nu=nu, dtype="float64"))
+        s.set_state(initial.to_spectral(initial.smooth_2d(n), 2))
+        s.advance(int(round(t_end / dt)), dt)
+        return s.get_state()
+
+    w_ref = np.fft.irfftn(solve(n_ref), s=(n_ref, n_ref), axes=(0, 1))
+    errs = []
+    for n in ns:
+        w = np.fft.irfftn(pad_spectrum(solve(n), n_ref), s=(n_ref, n_ref), axes=(0, 1))
+        errs.append(float(np.abs(w - w_ref).max() / np.abs(w_ref).max()))
+    return {"variant": variant, "n": list(ns), "err": errs, "n_ref": n_ref, "nu": nu,
+            "t_end": t_end, "dt": dt}
 
 
 def main(argv: list[str] | None = None) -> int:

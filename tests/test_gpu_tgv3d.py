@@ -53,3 +53,29 @@ def test_ifrk4_self_convergence_is_fourth_order_on_the_device(variant):
     r = temporal_convergence(variant)
     assert 3.8 < r["order"] < 4.3, r
     assert r["err"][-1] < 1e-8
+
+
+def test_spectral_convergence_in_n_matches_the_oracle():
+    """validation.py:103-119 on the device (fp64): the error against the 192^2 run falls
+    exponentially with n, and every grid's error equals the oracle's (its states agree to
+    round-off)."""
+    from oracle.numpy_oracle import OracleSolver
+    from pyspectral_b200 import initial
+    from pyspectral_b200.validation import pad_spectrum, spatial_convergence
+
+    r = spatial_convergence("b200/fused-inplace-graph")
+
+    def solve(n):
+        s = OracleSolver(n, 2, nu=r["nu"])
+        s.set_state(initial.to_spectral(initial.smooth_2d(n), 2))
+        s.advance(int(round(r["t_end"] / r["dt"])), r["dt"])
+        return s.get_state()
+
+    n_ref = r["n_ref"]
+    w_ref = np.fft.irfftn(solve(n_ref), s=(n_ref, n_ref), axes=(0, 1))
+    for n, e in zip(r["n"], r["err"]):
+        w = np.fft.irfftn(pad_spectrum(solve(n), n_ref), s=(n_ref, n_ref), axes=(0, 1))
+        want = float(np.abs(w - w_ref).max() / np.abs(w_ref).max())
+        assert abs(e - want) <= 1e-3 * want + 1e-12, (n, e, want)
+    err = dict(zip(r["n"], r["err"]))
+    assert err[64] < 1e-9 < err[32] < err[16]
