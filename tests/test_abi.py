@@ -79,3 +79,20 @@ def test_create_rejects_bad_arguments(lib):
     assert lib.sp_step(None, 0.1, None) == -1
     assert lib.sp_set_graph(None, 1) == -1
     assert lib.sp_last_error(None) == b"null handle"
+
+
+def test_streaming_switch_and_probe_arguments(lib):
+    """Host-side behaviour of the fused engine's pass switch and of the failure-path probe:
+    the switch round-trips without a device; the probe rejects its poll counts before any
+    CUDA call."""
+    prev = lib.sp_column_streaming()
+    assert prev == 1  # the streamed column pass is the default
+    try:
+        assert lib.sp_set_column_streaming(0) == 0 and lib.sp_column_streaming() == 0
+        assert lib.sp_set_column_streaming(1) == 0 and lib.sp_column_streaming() == 1
+    finally:
+        lib.sp_set_column_streaming(prev)
+    assert lib.sp_wait_probe(0, None) == -1
+    assert lib.sp_wait_probe((1 << 20) + 1, None) == -1
+    assert b"polls" in lib.sp_create_error()
+    assert lib.sp_take_device_error(None) == -1
