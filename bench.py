@@ -353,13 +353,18 @@ def ours_big3d(args, w: dict) -> int:
     ic = None
     gc.collect()  # the solver's diagnostics refer back to it
     torch.cuda.empty_cache()
-    b = make_solver(variant, cfg.with_(dtype="float64"))
-    b.set_state(tgv3d_device(n, torch.complex128))
-    b.step(h)
-    ub = b.state_native()
-    num = max(float((ua[c].to(torch.complex128) - ub[c]).abs().max()) for c in range(3))
-    rel_err = num / float(ub.abs().max())
-    del b, ua, ub
+    rel_err = None
+    try:  # the fp64 lean engine at 1024^3 holds about 100 GB more
+        b = make_solver(variant, cfg.with_(dtype="float64"))
+        b.set_state(tgv3d_device(n, torch.complex128))
+        b.step(h)
+        ub = b.state_native()
+        num = max(float((ua[c].to(torch.complex128) - ub[c]).abs().max()) for c in range(3))
+        rel_err = num / float(ub.abs().max())
+        del b, ub
+    except torch.OutOfMemoryError as e:  # reported, not fatal: the timed numbers stand
+        print(f"one-step fp64 check skipped: {e}", file=sys.stderr)
+    del ua
     gc.collect()
     torch.cuda.empty_cache()
 
