@@ -407,7 +407,9 @@ int sp_run_to(sp_solver* s, double t_end, double cfl, double dt_max, int cfl_eve
  *   - Scratch: a file-scope __device__ array of SP_NOALLOC_MAX_SHELLS doubles, held by every GPU
  *     that loads the library until the process exits.  Each call clears the shells it uses.
  *   - The first call on a device looks the array's device address up (cudaGetSymbolAddress, with
- *     that device current) and caches it; make that first call before any stream capture.
+ *     that device current) and caches it; make that first call before any stream capture.  The
+ *     cached address belongs to the device's primary context: after cudaDeviceReset (or any
+ *     tear-down of that context) this entry point must not be called again in the process.
  *   - Calls share the array: two calls whose work overlaps on the GPU race and give wrong
  *     results; order them on one stream.
  *   - Returns SP_ERR_ARG (message in sp_create_error()) when nshell does not match n and dim, or

@@ -34,7 +34,8 @@ static __device__ __align__(256) double g_noalloc_shells[SP_NOALLOC_MAX_SHELLS];
 
 // Device address of g_noalloc_shells per device.  In host code the array's name is only a
 // host-side stand-in, not a device address, so it is looked up with cudaGetSymbolAddress once
-// per device (with that device current) and cached.
+// per device (with that device current) and cached.  The cache is never invalidated: a caller
+// that resets the device (cudaDeviceReset) must not call this entry point afterwards.
 constexpr int kMaxDevices = 64;
 std::mutex g_lookup_mutex;
 double* g_shells_addr[kMaxDevices] = {};

@@ -48,8 +48,10 @@ class Comm:
         self.device = device  # where collective buffers live (a CUDA device for NCCL)
 
     def all_gather_rows(self, local: np.ndarray, counts: Sequence[int]) -> list[np.ndarray]:
-        """Every rank's (counts[r], k) float64 rows; each rank passes its own."""
-        if self.world == 1:
+        """Every rank's (counts[r], k) float64 rows; each rank passes its own.  Without a
+        process group the rows are returned as they are; with one (of any size, one rank
+        included) they go through the group's ``all_gather``."""
+        if self.dist is None:
             return [np.asarray(local, dtype=np.float64)]
         import torch
 
@@ -63,10 +65,12 @@ class Comm:
         return [o.cpu().numpy()[: counts[r]] for r, o in enumerate(out)]
 
     def allreduce_mean_(self, t: Any) -> Any:
-        """In-place mean of a tensor over the ranks."""
-        if self.world > 1:
+        """In-place mean of a tensor over the ranks (the group's ``all_reduce`` whenever a
+        process group exists, one rank included)."""
+        if self.dist is not None:
             self.dist.all_reduce(t)
-            t /= self.world
+            if self.world > 1:
+                t /= self.world
         return t
 
 

@@ -30,9 +30,13 @@ _NSIZE = 8  # sp_slab_query_sizes entries
 
 def exchange_blocks(recv: Any, send: Any, block_bytes: int, nranks: int, comm: Any) -> None:
     """All-to-all of ``nranks`` equal contiguous blocks: block p of this rank's ``send`` lands
-    in block (this rank) of rank p's ``recv`` (``comm``: torch.distributed, NCCL on GPUs)."""
+    in block (this rank) of rank p's ``recv`` (``comm``: torch.distributed, NCCL on GPUs).
+    Without ``comm`` a single rank's exchange is a device copy; with ``comm`` the collective runs
+    for any number of ranks, one included."""
     nb = nranks * block_bytes
-    if nranks == 1:
+    if comm is None:
+        if nranks != 1:
+            raise ValueError("an exchange between several ranks needs a process group")
         if recv.data_ptr() != send.data_ptr():
             recv[:nb].copy_(send[:nb])
         return
@@ -77,8 +81,10 @@ class SlabSolver:
         u8 = dict(dtype=torch.uint8, device=self.device)
         self.W = torch.zeros(int(sz[2]), **u8)
         self.send = torch.zeros(int(sz[3]), **u8)
-        # one rank: the all-to-all is the identity, so receive where the blocks were packed
-        self.recv = self.send if self.nranks == 1 else torch.zeros(int(sz[3]), **u8)
+        # one rank without a process group: the all-to-all is the identity, so receive where
+        # the blocks were packed; through a process group the collective needs its own buffer
+        self.recv = (self.send if self.nranks == 1 and comm is None
+                     else torch.zeros(int(sz[3]), **u8))
         self.aux = torch.zeros(int(sz[4]), **u8)
         self.ws = torch.empty(max(1, int(sz[5])), **u8)
         self._check(lib.sp_slab_bind(h, _lib.dptr(self.u0), _lib.dptr(self.acc), _lib.dptr(self.W),

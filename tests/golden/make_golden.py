@@ -1,9 +1,8 @@
 """Generate tests/golden/reference_vectors.npz by running the reference implementation.
 
-Run in a checkout where pyspectral's sources are available (default: /root/reference/src, or
-set PYSPECTRAL_SRC):
+Run where pyspectral's sources are available, with PYSPECTRAL_SRC naming its src/ directory:
 
-    python tests/golden/make_golden.py
+    PYSPECTRAL_SRC=/path/to/pyspectral/src python tests/golden/make_golden.py
 
 Every array is produced by pyspectral itself (NumpySolver, Diagnostics, initial, validation):
 the cross-backend parity protocol of tests/test_backends.py:24-47 (forcing and dt changes), the
@@ -20,7 +19,9 @@ from pathlib import Path
 
 import numpy as np
 
-SRC = os.environ.get("PYSPECTRAL_SRC", "/root/reference/src")
+SRC = os.environ.get("PYSPECTRAL_SRC")
+if not SRC:
+    sys.exit("set PYSPECTRAL_SRC to pyspectral's src/ directory")
 sys.path.insert(0, SRC)
 
 from pyspectral import initial  # noqa: E402

@@ -208,15 +208,16 @@ def test_run_steps_is_cfl_every_10():
 # ----------------------------------------------------------------------------- pyspectral plugin
 def _pyspectral_importable() -> bool:
     import importlib.util
+    import os
     import sys
 
-    src = "/root/reference/src"
-    if importlib.util.find_spec("pyspectral") is None and Path(src).exists():
+    src = os.environ.get("PYSPECTRAL_SRC", "")  # pyspectral's src/ directory, when available
+    if importlib.util.find_spec("pyspectral") is None and src and Path(src).exists():
         sys.path.append(src)
     return importlib.util.find_spec("pyspectral") is not None
 
 
-@pytest.mark.skipif(not _pyspectral_importable(), reason="pyspectral not importable here")
+@pytest.mark.skipif(not _pyspectral_importable(), reason="pyspectral not importable (set PYSPECTRAL_SRC to its src/ directory)")
 def test_plugin_registers_into_pyspectral_registry(capsys):
     from pyspectral.backends import REGISTRY as REF, BackendUnavailable as RefUnavailable
     from pyspectral.backends import get as ref_get
@@ -248,7 +249,7 @@ def test_plugin_registers_into_pyspectral_registry(capsys):
         del REF[before:]
 
 
-@pytest.mark.skipif(not _pyspectral_importable(), reason="pyspectral not importable here")
+@pytest.mark.skipif(not _pyspectral_importable(), reason="pyspectral not importable (set PYSPECTRAL_SRC to its src/ directory)")
 def test_plugin_class_raises_pyspectral_unavailable():
     from pyspectral.backends.base import BackendUnavailable as RefUnavailable
     from pyspectral.config import Config as RefConfig

@@ -4,6 +4,7 @@ driver (src/pyspectral/simulate.py:40-96 with NumpySolver), and the dissipation 
 from __future__ import annotations
 
 import importlib.util
+import os
 import sys
 from pathlib import Path
 
@@ -14,16 +15,17 @@ from oracle.numpy_oracle import OracleSolver, run_cfl
 from pyspectral_b200 import initial
 from pyspectral_b200.validation import TGV_NU, compare_dissipation
 
-_SRC = "/root/reference/src"
+# pyspectral's source tree (its src/ directory), when the reference itself is available
+_SRC = os.environ.get("PYSPECTRAL_SRC", "")
 
 
 def _reference_importable() -> bool:
-    if importlib.util.find_spec("pyspectral") is None and Path(_SRC).exists():
+    if importlib.util.find_spec("pyspectral") is None and _SRC and Path(_SRC).exists():
         sys.path.append(_SRC)
     return importlib.util.find_spec("pyspectral") is not None
 
 
-@pytest.mark.skipif(not _reference_importable(), reason="pyspectral not importable here")
+@pytest.mark.skipif(not _reference_importable(), reason="pyspectral not importable (set PYSPECTRAL_SRC to its src/ directory)")
 @pytest.mark.parametrize("form", ["rotational", "basdevant"])
 def test_oracle_run_loop_matches_the_reference_driver(form):
     from pyspectral.backends.numpy_ref import NumpySolver

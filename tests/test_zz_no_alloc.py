@@ -49,6 +49,25 @@ def test_noalloc_spectrum_matches_regular_twice(dim, n, dtype):
     assert got.sum() == pytest.approx(s.diag.energy(s.state_native()), rel=1e-12)
 
 
+def test_noalloc_spectrum_large_grid_accumulates_in_the_array_itself():
+    """Above 6144 shells the histogram no longer fits the kernel's shared memory and every
+    block adds straight into the file-scope array: 8704^2 fp32 (6156 shells), twice in a row,
+    so the clearing of that path is checked too."""
+    from pyspectral_b200 import Config, initial
+    from pyspectral_b200.registry import get
+
+    n = 8704
+    s = get("b200").make(Config(n=n, dim=2, dtype="float32", nu=1e-5))
+    s.set_state(initial.random_phase_2d(n, k0=40, seed=5))
+    k, regular = s.diag.spectrum(s.state_native())
+    nshell = len(regular)
+    assert nshell > 6144
+    for _ in range(2):
+        st, got = _noalloc(s.lib, s.state_native(), n, 2, False, nshell, s._stream())
+        assert st == 0, s.lib.sp_create_error()
+        np.testing.assert_allclose(got, regular, rtol=1e-12, atol=1e-300)
+
+
 def test_noalloc_spectrum_rejects_sizes_beyond_its_array():
     import torch
 
