@@ -174,4 +174,7 @@ def check_device_errors(lib: ctypes.CDLL) -> None:
         raise EngineError(f"sp_take_device_error failed: {STATUS_NAMES.get(st, st)}")
     if bits.value:
         raise EngineError(f"device error bits {bits.value:#x}: a streamed column pass timed out "
-                          "waiting for its TMA data; the state is invalid")
+                          "waiting for its TMA data; the state is invalid, and bulk copies into "
+                          "the timed-out block's shared memory may still have been in flight "
+                          "when it exited: recreate the solver (a new process is the safe "
+                          "choice)")

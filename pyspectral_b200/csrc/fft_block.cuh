@@ -229,6 +229,15 @@ struct FftPlan {
     static constexpr int TW_SIZE = tw_offset(false, NP) > 0 ? tw_offset(false, NP) : 1;
 };
 
+// Barrier between the passes of a transform: the whole CTA, or (WARP) only the calling warp,
+// for kernels whose every sequence lies inside one warp (n <= 512) and whose warps exchange
+// through buffers of their own.
+template <bool WARP>
+__device__ __forceinline__ void seq_sync() {
+    if constexpr (WARP) __syncwarp();
+    else __syncthreads();
+}
+
 // shared-memory index with one pad element every 16 (conflict-free strided access)
 __device__ __forceinline__ int spad(int e) { return e + (e >> 4); }
 
@@ -296,89 +305,64 @@ __device__ __forceinline__ void pass_compute(E (&v)[16], int t, const C* __restr
     }
 }
 
+// Padded addresses with compile-time offsets.  A pass reads element t + c (c = T g + m N/R) and
+// a pass writes element b_t + c (c = T g R + m S, b_t = (t / S) S R + (t mod S)).  Whenever the
+// 16-element blocks of c line up (c's part from g a multiple of 16), spad(b + c) =
+// spad(b) + c + c / 16, because b's low four bits plus c's never carry: for S >= 16 c's low
+// bits are zero; for S < 16, b mod 16 < S when S R >= 16 (m S mod 16 <= 16 - S), and for S = 1,
+// b = R t is a multiple of R with m < R.  Each thread then forms one padded base per exchange
+// and every access is that base plus an immediate.
+template <int R, int S>
+constexpr bool blocks_line_up() { return S >= 16 || S * R >= 16 || S == 1; }
+
 template <int N, int R, typename E>
 __device__ __forceinline__ void pass_load(E (&v)[16], const E* sm, int t) {
     constexpr int G = 16 / R;
+    constexpr int T = N / 16;
+    const E* st = sm + spad(t);
 #pragma unroll
     for (int g = 0; g < G; ++g)
 #pragma unroll
-        for (int m = 0; m < R; ++m) v[g * R + m] = sm[spad(in_pos<N, R>(t, g, m))];
+        for (int m = 0; m < R; ++m) {
+            const int c = T * g + m * (N / R);  // a constant once unrolled
+            v[g * R + m] = (c % 16 == 0) ? st[c + (c >> 4)] : sm[spad(t + c)];
+        }
 }
 
 template <int N, int R, int S, typename E>
 __device__ __forceinline__ void pass_store(const E (&v)[16], E* sm, int t) {
     constexpr int G = 16 / R;
     constexpr int T = N / 16;
+    if constexpr ((T % S == 0 || G == 1) && blocks_line_up<R, S>()) {
+        const int bt = (t / S) * S * R + (t & (S - 1));
+        E* sb = sm + spad(bt);
 #pragma unroll
-    for (int g = 0; g < G; ++g) {
-        const int j = t + T * g;
-        const int base = (j / S) * S * R + (j & (S - 1));
+        for (int g = 0; g < G; ++g)
 #pragma unroll
-        for (int m = 0; m < R; ++m) sm[spad(base + m * S)] = v[g * R + m];
-    }
-}
-
-// Full transform.  On entry v holds the input in the pattern of pass 0 (in_pos with radix
-// radix(INV, 0)); on exit v holds the output at in_pos with the last pass's radix.  `sm` is this
-// sequence's padded shared buffer; every thread of the CTA must call (barriers inside).
-template <int N, bool INV, typename E, typename C>
-__device__ __forceinline__ void block_fft(E (&v)[16], E* sm, int t, const C* __restrict__ tw) {
-    using P = FftPlan<N>;
-    constexpr int DIR = INV ? 1 : -1;
-    constexpr int R0 = P::radix(INV, 0), S0 = P::stride(INV, 0);
-    pass_compute<N, R0, S0, DIR>(v, t, tw);  // S0 = 1: no twiddles
-    if constexpr (P::NP > 1) {
-        constexpr int R1 = P::radix(INV, 1), S1 = P::stride(INV, 1);
-        pass_store<N, R0, S0>(v, sm, t);
-        __syncthreads();
-        pass_load<N, R1>(v, sm, t);
-        __syncthreads();
-        pass_compute<N, R1, S1, DIR>(v, t, tw + P::tw_offset(INV, 1));
-        if constexpr (P::NP > 2) {
-            constexpr int R2 = P::radix(INV, 2), S2 = P::stride(INV, 2);
-            pass_store<N, R1, S1>(v, sm, t);
-            __syncthreads();
-            pass_load<N, R2>(v, sm, t);
-            __syncthreads();
-            pass_compute<N, R2, S2, DIR>(v, t, tw + P::tw_offset(INV, 2));
-            if constexpr (P::NP > 3) {
-                constexpr int R3 = P::radix(INV, 3), S3 = P::stride(INV, 3);
-                pass_store<N, R2, S2>(v, sm, t);
-                __syncthreads();
-                pass_load<N, R3>(v, sm, t);
-                __syncthreads();
-                pass_compute<N, R3, S3, DIR>(v, t, tw + P::tw_offset(INV, 3));
+            for (int m = 0; m < R; ++m) {
+                const int c = T * g * R + m * S;
+                if ((T * g * R) % 16 == 0) sb[c + (c >> 4)] = v[g * R + m];
+                else sm[spad(bt + c)] = v[g * R + m];
             }
+    } else {
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const int j = t + T * g;
+            const int base = (j / S) * S * R + (j & (S - 1));
+#pragma unroll
+            for (int m = 0; m < R; ++m) sm[spad(base + m * S)] = v[g * R + m];
         }
     }
 }
 
-// Exchange between two passes of a Pair transform through a buffer of single complex values
-// (half the bytes of a Pair buffer): the `a` sequences move first, then the `b` sequences.
-template <int N, int R0, int S0, int R1, typename T>
-__device__ __forceinline__ void exchange_halves(Pair<T> (&v)[16], cplx<T>* sm, int t) {
-    constexpr int G0 = 16 / R0, G1 = 16 / R1;
-    constexpr int TT = N / 16;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-#pragma unroll
-        for (int g = 0; g < G0; ++g) {
-            const int j = t + TT * g;
-            const int base = (j / S0) * S0 * R0 + (j & (S0 - 1));
-#pragma unroll
-            for (int m = 0; m < R0; ++m)
-                sm[spad(base + m * S0)] = h == 0 ? v[g * R0 + m].a : v[g * R0 + m].b;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int g = 0; g < G1; ++g)
-#pragma unroll
-            for (int m = 0; m < R1; ++m) {
-                const cplx<T> e = sm[spad(in_pos<N, R1>(t, g, m))];
-                if (h == 0) v[g * R1 + m].a = e;
-                else v[g * R1 + m].b = e;
-            }
-        __syncthreads();
+// Group G of pass_radix2_half and the groups after it, each rotation formed where it is used
+// (fewer live registers than forming all eight first).
+template <int DIR, int G, typename E, typename C>
+__device__ __forceinline__ void radix2_half_group(E (&v)[16], const C w1) {
+    if constexpr (G < 8) {
+        v[G * 2 + 1] = emul(v[G * 2 + 1], rot16<DIR, G>(w1));
+        dft2<DIR>(v + G * 2);
+        radix2_half_group<DIR, G + 1>(v, w1);
     }
 }
 
@@ -388,20 +372,7 @@ __device__ __forceinline__ void exchange_halves(Pair<T> (&v)[16], cplx<T>* sm, i
 template <int N, int DIR, typename E, typename C>
 __device__ __forceinline__ void pass_radix2_half(E (&v)[16], int t, const C* __restrict__ tw) {
     const C w1 = tw_load<DIR>(tw, t);
-    C w[8];
-    w[0] = w1;
-    w[1] = rot16<DIR, 1>(w1);
-    w[2] = rot16<DIR, 2>(w1);
-    w[3] = rot16<DIR, 3>(w1);
-    w[4] = rot16<DIR, 4>(w1);
-    w[5] = rot16<DIR, 5>(w1);
-    w[6] = rot16<DIR, 6>(w1);
-    w[7] = rot16<DIR, 7>(w1);
-#pragma unroll
-    for (int g = 0; g < 8; ++g) {
-        v[g * 2 + 1] = emul(v[g * 2 + 1], w[g]);
-        dft2<DIR>(v + g * 2);
-    }
+    radix2_half_group<DIR, 0>(v, w1);
 }
 
 // pass_compute, with pass_radix2_half for the radix-2 pass at stride N/2.
@@ -411,9 +382,66 @@ __device__ __forceinline__ void pass_compute_h(E (&v)[16], int t, const C* __res
     else pass_compute<N, R, S, DIR>(v, t, tw);
 }
 
+// Full transform.  On entry v holds the input in the pattern of pass 0 (in_pos with radix
+// radix(INV, 0)); on exit v holds the output at in_pos with the last pass's radix.  `sm` is this
+// sequence's padded shared buffer; every thread of the CTA must call (barriers inside).
+template <int N, bool INV, bool WARP = false, typename E, typename C>
+__device__ __forceinline__ void block_fft(E (&v)[16], E* sm, int t, const C* __restrict__ tw) {
+    using P = FftPlan<N>;
+    static_assert(!WARP || P::T <= 32, "a warp-synchronised transform fits in one warp");
+    constexpr int DIR = INV ? 1 : -1;
+    constexpr int R0 = P::radix(INV, 0), S0 = P::stride(INV, 0);
+    pass_compute<N, R0, S0, DIR>(v, t, tw);  // S0 = 1: no twiddles
+    if constexpr (P::NP > 1) {
+        constexpr int R1 = P::radix(INV, 1), S1 = P::stride(INV, 1);
+        pass_store<N, R0, S0>(v, sm, t);
+        seq_sync<WARP>();
+        pass_load<N, R1>(v, sm, t);
+        seq_sync<WARP>();
+        pass_compute_h<N, R1, S1, DIR>(v, t, tw + P::tw_offset(INV, 1));
+        if constexpr (P::NP > 2) {
+            constexpr int R2 = P::radix(INV, 2), S2 = P::stride(INV, 2);
+            pass_store<N, R1, S1>(v, sm, t);
+            seq_sync<WARP>();
+            pass_load<N, R2>(v, sm, t);
+            seq_sync<WARP>();
+            pass_compute_h<N, R2, S2, DIR>(v, t, tw + P::tw_offset(INV, 2));
+            if constexpr (P::NP > 3) {
+                constexpr int R3 = P::radix(INV, 3), S3 = P::stride(INV, 3);
+                pass_store<N, R2, S2>(v, sm, t);
+                seq_sync<WARP>();
+                pass_load<N, R3>(v, sm, t);
+                seq_sync<WARP>();
+                pass_compute_h<N, R3, S3, DIR>(v, t, tw + P::tw_offset(INV, 3));
+            }
+        }
+    }
+}
+
+// Exchange between two passes of a Pair transform through a buffer of single complex values
+// (half the bytes of a Pair buffer): the `a` sequences move first, then the `b` sequences.
+template <int N, int R0, int S0, int R1, bool WARP = false, typename T>
+__device__ __forceinline__ void exchange_halves(Pair<T> (&v)[16], cplx<T>* sm, int t) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        cplx<T> u[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) u[e] = h == 0 ? v[e].a : v[e].b;
+        pass_store<N, R0, S0>(u, sm, t);
+        seq_sync<WARP>();
+        pass_load<N, R1>(u, sm, t);
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            if (h == 0) v[e].a = u[e];
+            else v[e].b = u[e];
+        }
+        seq_sync<WARP>();
+    }
+}
+
 // block_fft of Pair elements with the exchanges of exchange_halves: `sm` holds
 // FftPlan<N>::SMEM complex values instead of Pairs.
-template <int N, bool INV, typename T, typename C>
+template <int N, bool INV, bool WARP = false, typename T, typename C>
 __device__ __forceinline__ void block_fft_halves(Pair<T> (&v)[16], cplx<T>* sm, int t,
                                                  const C* __restrict__ tw) {
     using P = FftPlan<N>;
@@ -422,15 +450,15 @@ __device__ __forceinline__ void block_fft_halves(Pair<T> (&v)[16], cplx<T>* sm, 
     pass_compute<N, R0, S0, DIR>(v, t, tw);
     if constexpr (P::NP > 1) {
         constexpr int R1 = P::radix(INV, 1), S1 = P::stride(INV, 1);
-        exchange_halves<N, R0, S0, R1>(v, sm, t);
+        exchange_halves<N, R0, S0, R1, WARP>(v, sm, t);
         pass_compute_h<N, R1, S1, DIR>(v, t, tw + P::tw_offset(INV, 1));
         if constexpr (P::NP > 2) {
             constexpr int R2 = P::radix(INV, 2), S2 = P::stride(INV, 2);
-            exchange_halves<N, R1, S1, R2>(v, sm, t);
+            exchange_halves<N, R1, S1, R2, WARP>(v, sm, t);
             pass_compute_h<N, R2, S2, DIR>(v, t, tw + P::tw_offset(INV, 2));
             if constexpr (P::NP > 3) {
                 constexpr int R3 = P::radix(INV, 3), S3 = P::stride(INV, 3);
-                exchange_halves<N, R2, S2, R3>(v, sm, t);
+                exchange_halves<N, R2, S2, R3, WARP>(v, sm, t);
                 pass_compute_h<N, R3, S3, DIR>(v, t, tw + P::tw_offset(INV, 3));
             }
         }

@@ -74,6 +74,48 @@ __device__ __forceinline__ cplx<T> row_input(const Pair<T>* __restrict__ X, int 
     return mk<T>(0, 0);
 }
 
+// The same for register slot M of the first inverse pass (radix 16: slot M of thread t holds
+// k = t + M n/16), with the kept columns kc = (n + 2) / 3 known at compile time: each slot's
+// k range lies wholly in the low half spectrum, the dealiased gap (zero) or the high half for
+// all but the two slots straddling +-kc, so the branches and zeros resolve when compiled.
+// Xr: the row's first element, X + (p kc) 2 + half; column k is Xr[2 k].
+template <typename T, int N, int M>
+__device__ __forceinline__ cplx<T> row_input_slot(const Pair<T>* __restrict__ Xr, int t) {
+    constexpr int KC = (N + 2) / 3;
+    constexpr int L = N / 16;
+    constexpr int LO = M * L, HI = LO + L - 1;  // k range of the slot
+    const int k = t + LO;
+    auto low = [&](int kk) {
+        Pair<T> q = Xr[2 * kk];
+        if (M == 0 && kk == 0) return mk<T>(q.a.x, q.b.x);  // c2r ignores Im at k = 0
+        return mk<T>(q.a.x - q.b.y, q.a.y + q.b.x);
+    };
+    auto high = [&](int kk) {
+        Pair<T> q = Xr[2 * (N - kk)];
+        return mk<T>(q.a.x + q.b.y, q.b.x - q.a.y);
+    };
+    if constexpr (HI < KC) {
+        return low(k);
+    } else if constexpr (LO > N - KC) {
+        return high(k);
+    } else if constexpr (LO >= KC && HI <= N - KC) {
+        return mk<T>(0, 0);
+    } else {
+        if (k < KC) return low(k);
+        if (k > N - KC) return high(k);
+        return mk<T>(0, 0);
+    }
+}
+
+template <typename T, int N, int M = 0>
+__device__ __forceinline__ void row_inputs(cplx<T> (&v)[16], const Pair<T>* __restrict__ Xr,
+                                           int t) {
+    if constexpr (M < 16) {
+        v[M] = row_input_slot<T, N, M>(Xr, t);
+        row_inputs<T, N, M + 1>(v, Xr, t);
+    }
+}
+
 // Row pairs per CTA: the sub-block structure of Fused2D over n/2 row pairs.
 template <int N>
 struct RowPairs {
@@ -110,12 +152,10 @@ __global__ void __launch_bounds__(RowSingle<N, BX>::THREADS, 2) k_row_pass(
     const int p = row >> 1, half = row & 1;
     X += blockIdx.y * x_stride;
 
+    static_assert(RI == 16, "first inverse pass is radix 16: slot m holds k = t + m n/16");
+    constexpr int KC = (N + 2) / 3;  // == kc: the dealiased columns, fixed by n
     cplx<T> v[16];
-#pragma unroll
-    for (int g = 0; g < 16 / RI; ++g)
-#pragma unroll
-        for (int m = 0; m < RI; ++m)
-            v[g * RI + m] = row_input<T, N>(X, p, in_pos<N, RI>(t, g, m), kc, half);
+    row_inputs<T, N>(v, X + (size_t)p * KC * 2 + half, t);
     block_fft<N, true>(v, sm, t, tw);
     // physical space: z = u + i v  ->  (v^2 - u^2) + i (u v)
 #pragma unroll
@@ -126,18 +166,40 @@ __global__ void __launch_bounds__(RowSingle<N, BX>::THREADS, 2) k_row_pass(
     __syncthreads();
     block_fft<N, false>(v, sm, t, tw);
     __syncthreads();
+    static_assert(RF == 16, "last forward pass is radix 16: slot m holds k = t + m n/16");
+    {
+        cplx<T>* st = sm + spad(t);
 #pragma unroll
-    for (int g = 0; g < 16 / RF; ++g)
-#pragma unroll
-        for (int m = 0; m < RF; ++m) sm[spad(in_pos<N, RF>(t, g, m))] = v[g * RF + m];
+        for (int m = 0; m < 16; ++m) {
+            const int c = m * TT;
+            if (c % 16 == 0) st[c + (c >> 4)] = v[m];
+            else sm[spad(t + c)] = v[m];
+        }
+    }
     __syncthreads();
     // P(k) = (Z'(k) + conj Z'(n-k)) / 2, Q(k) = (Z'(k) - conj Z'(n-k)) / 2i
-    for (int k = t; k < kc; k += TT) {
-        cplx<T> a = sm[spad(k)], b = sm[spad((N - k) & (N - 1))];
-        Pair<T> o;
-        o.a = mk<T>((T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y));
-        o.b = mk<T>((T)0.5 * (a.y + b.y), (T)0.5 * (b.x - a.x));
-        X[((size_t)p * kc + k) * 2 + half] = o;
+    Pair<T>* Xo = X + (size_t)p * KC * 2 + half;
+    // n - k = (n - (j+1) TT) + (TT - t): a padded base for TT - t plus a constant (TT a
+    // multiple of 16); k = 0 (t = 0, j = 0) reads element 0
+    const int pk = spad(t), pnk = spad(TT - t);
+#pragma unroll
+    for (int j = 0; j < (KC + TT - 1) / TT; ++j) {
+        const int k = t + j * TT;
+        if ((j + 1) * TT <= KC || k < KC) {
+            cplx<T> a, b;
+            if constexpr (TT % 16 == 0) {
+                const int ca = j * TT, cb = N - (j + 1) * TT;
+                a = sm[pk + ca + (ca >> 4)];
+                b = sm[(j == 0 && t == 0) ? 0 : pnk + cb + (cb >> 4)];
+            } else {
+                a = sm[spad(k)];
+                b = sm[spad((N - k) & (N - 1))];
+            }
+            Pair<T> o;
+            o.a = mk<T>((T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y));
+            o.b = mk<T>((T)0.5 * (a.y + b.y), (T)0.5 * (b.x - a.x));
+            Xo[2 * k] = o;
+        }
     }
 }
 
@@ -198,6 +260,15 @@ __global__ void __launch_bounds__(RowPairs<N>::THREADS) k_row_max(const Pair<T>*
     }
 }
 
+// Streaming store of one Pair (written once, read by the next pass: not kept in L1).
+__device__ __forceinline__ void st_stream(Pair<float>* p, const Pair<float>& v) {
+    __stcs(reinterpret_cast<float4*>(p), make_float4(v.a.x, v.a.y, v.b.x, v.b.y));
+}
+__device__ __forceinline__ void st_stream(Pair<double>* p, const Pair<double>& v) {
+    __stcs(reinterpret_cast<double2*>(p), v.a);
+    __stcs(reinterpret_cast<double2*>(p) + 1, v.b);
+}
+
 // ------------------------------------------------------------------------------- column pass
 // Next inverse-FFT inputs (u, v) of a vorticity mode, scaled and dealiased (velocity2).
 template <typename T>
@@ -232,17 +303,17 @@ __device__ __forceinline__ void col_update(Pair<T> (&v)[16], int t, int ky, bool
             cplx<T> nxt = mk<T>(0, 0);
             if (keep) {
                 const size_t o = (size_t)ky * N + i;
-                cplx<T> U = u0t[o];
+                cplx<T> U = __ldcs(u0t + o);  // streamed once: keep L1 for the twiddles
                 if constexpr (STAGE < 0) {
                     nxt = U;
                 } else {
                     Pair<T> e = v[g * RL + m];
                     cplx<T> Nl = axpy(kx * kyr, e.a, scl(kx * kx - kyr * kyr, e.b));
                     IFac<T> f = if_factors(tab, nh, akx, ky, -1, k2, p);
-                    cplx<T> C = STAGE > 0 ? acct[o] : mk<T>(0, 0);
+                    cplx<T> C = STAGE > 0 ? __ldcs(acct + o) : mk<T>(0, 0);
                     nxt = lawson_stage<T, (STAGE < 0 ? 0 : STAGE)>(p.dt, f, Nl, U, C);
-                    if (STAGE == 3) u0t[o] = nxt;
-                    else acct[o] = C;
+                    if (STAGE == 3) __stcs(u0t + o, nxt);
+                    else __stcs(acct + o, C);
                 }
             }
             v[g * RL + m] = next_inputs<T>(kx, kyr, k2, keep, nxt, p.scale);
@@ -405,7 +476,8 @@ k_col_stream(const __grid_constant__ CUtensorMap xmap, Pair<T>* __restrict__ X, 
 #pragma unroll
         for (int g = 0; g < 16 / RIL; ++g)
 #pragma unroll
-            for (int m = 0; m < RIL; ++m) X[xidx(in_pos<N, RIL>(t, g, m), ky, kc)] = v[g * RIL + m];
+            for (int m = 0; m < RIL; ++m)
+                st_stream(X + xidx(in_pos<N, RIL>(t, g, m), ky, (N + 2) / 3), v[g * RIL + m]);
     }
 }
 

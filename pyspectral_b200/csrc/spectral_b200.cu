@@ -20,6 +20,7 @@
 #include "spectral_b200.h"
 #include "closure.cuh"
 #include "fused2d.h"
+#include "fused3d.h"
 #include "pointwise.cuh"
 #include "reduce.cuh"
 
@@ -86,6 +87,8 @@ struct sp_solver {
     // whether the NumPy-layout state u0 reflects the transposed state
     int kc = 0;
     size_t work_bytes = 0, off_u0t = 0;
+    // fused 3D mode: the work array is B_spec followed (at off_bphys) by B_phys
+    size_t off_bphys = 0;
     bool u0_fresh = true;
     // cuFFT
     cufftHandle plan_inv = 0, plan_fwd = 0, plan_c2r1 = 0;
@@ -126,7 +129,11 @@ struct sp_solver {
     double* spec_dev() const { return (double*)((char*)aux + off_spec); }
     void* tw_dev() const { return (char*)aux + off_tw; }
     void* u0t_dev() const { return (char*)W + off_u0t; }
+    void* bphys_dev() const { return (char*)W + off_bphys; }
     bool fused() const { return fft_mode == SP_FFT_FUSED; }
+    bool fused2() const { return fused() && dim == 2; }
+    bool fused3() const { return fused() && dim == 3; }
+    int rot() const { return form == SP_FORM_ROTATIONAL ? 1 : 0; }
     bool cl() const { return closure != nullptr; }
 };
 
@@ -360,6 +367,39 @@ int fused_col(sp_solver* s, int stage, cudaStream_t st) {
 
 // Stage of a closure run whose network term is held from the step's first stage: the plain
 // velocity-pair transforms and products on work slots 1-2; slot 0 keeps the transformed term.
+// fused 3D: the four passes of a stage (Y inverse, Z, Y forward, X with the Lawson update)
+int fused3_phase(sp_solver* s, int phase, int stage, cudaStream_t st) {
+    switch (phase) {
+        case 0:
+            SP_CUDA(sp::fused3::y_inverse(s->n, s->fp64, s->rot(), s->W, s->bphys_dev(), s->ninv,
+                                          s->tw_dev(), st));
+            break;
+        case 1:
+            SP_CUDA(sp::fused3::z_pass(s->n, s->fp64, s->rot(), 0, s->bphys_dev(), s->tw_dev(),
+                                       s->umax_dev(), 0, st));
+            break;
+        case 2:
+            SP_CUDA(sp::fused3::y_forward(s->n, s->fp64, s->rot(), s->bphys_dev(), s->W, s->nfwd,
+                                          s->tw_dev(), st));
+            break;
+        default:
+            SP_CUDA(sp::fused3::x_pass(s->n, s->fp64, s->rot(), stage, s->W, s->u0, s->acc,
+                                       s->tab_dev(), s->params_dev(), s->tw_dev(), st));
+    }
+    s->launches += 1;
+    return SP_OK;
+}
+
+// fused 3D: max |u_i| of the live state into umax_dev()[0..3) (its stage-0 inputs are in B_spec)
+int fused3_umax(sp_solver* s, cudaStream_t st) {
+    SP_CUDA(sp::fused3::y_inverse(s->n, s->fp64, s->rot(), s->W, s->bphys_dev(), 3, s->tw_dev(),
+                                  st));
+    SP_CUDA(sp::fused3::z_pass(s->n, s->fp64, s->rot(), 1, s->bphys_dev(), s->tw_dev(),
+                               s->umax_dev(), 1, st));
+    s->launches += 2;
+    return SP_OK;
+}
+
 int held_closure_stage(sp_solver* s, cudaStream_t st) {
     char* Wuv = (char*)s->W + field_bytes(s);
     int r;
@@ -385,6 +425,14 @@ int run_step(sp_solver* s, cudaStream_t st) {
             }
             if ((r = run_post(s, stage, st))) return r;
         }
+        return SP_OK;
+    }
+    if (s->fused3()) {
+        for (int stage = 0; stage < 4; ++stage)
+            for (int phase = 0; phase < 4; ++phase) {
+                int r = fused3_phase(s, phase, stage, st);
+                if (r) return r;
+            }
         return SP_OK;
     }
     if (s->fused()) {
@@ -516,7 +564,10 @@ namespace {
 int enqueue_run_diag(sp_solver* s, bool need_umax, bool need_band, cudaStream_t st) {
     if (need_umax) {
         SP_CUDA(cudaMemsetAsync(s->umax_dev(), 0, 4 * sizeof(unsigned long long), st));
-        if (s->fused()) {
+        if (s->fused3()) {
+            int r = fused3_umax(s, st);
+            if (r) return r;
+        } else if (s->fused()) {
             SP_CUDA(sp::fused::row_max(s->n, s->fp64, s->W, s->kc, s->tw_dev(), s->umax_dev(), st));
             s->launches += 1;
         } else {
@@ -550,7 +601,7 @@ int enqueue_run_diag(sp_solver* s, bool need_umax, bool need_band, cudaStream_t 
         }
     }
     if (need_band) {
-        if (s->fused()) {
+        if (s->fused2()) {
             SP_CUDA(sp::fused::reduce_t(s->fp64, s->u0t_dev(), s->n, s->kc, 0, 1, s->klo, s->khi,
                                         s->partials_dev(), kRedBlocks, s->out_dev(), st));
             s->launches += 2;
@@ -667,9 +718,10 @@ sp_solver* sp_create(int n, int dim, int form, int fp64, int fft_mode, int* stat
         return set(SP_ERR_UNSUPPORTED, "2D supports the basdevant form only");
     if (fft_mode != SP_FFT_CUFFT && fft_mode != SP_FFT_CUFFT_LEAN && fft_mode != SP_FFT_FUSED)
         return set(SP_ERR_ARG, "unknown fft_mode");
-    if (fft_mode == SP_FFT_FUSED && dim != 2)
-        return set(SP_ERR_UNSUPPORTED, "the fused FFT engine runs 2D grids only");
-    if (fft_mode == SP_FFT_FUSED && !sp::fused::supported(n, fp64))
+    if (fft_mode == SP_FFT_FUSED && dim == 3 && !sp::fused3::supported(n, fp64))
+        return set(SP_ERR_UNSUPPORTED,
+                   "the fused 3D FFT engine needs n a power of two in 16..512");
+    if (fft_mode == SP_FFT_FUSED && dim == 2 && !sp::fused::supported(n, fp64))
         return set(SP_ERR_UNSUPPORTED,
                    "the fused FFT engine needs n a power of two in 16..8192 (fp32) or 16..4096 (fp64)");
     int nh = n / 2 + 1;
@@ -711,6 +763,18 @@ sp_solver* sp_create(int n, int dim, int form, int fp64, int fft_mode, int* stat
     s->aux_bytes = off;
     s->work_bytes = (size_t)s->nwork * field_bytes(s);
 
+    if (fft_mode == SP_FFT_FUSED && dim == 3) {
+        const int rot = form == SP_FORM_ROTATIONAL ? 1 : 0;
+        s->off_bphys = align256(sp::fused3::spec_bytes(n, fp64, rot));
+        s->work_bytes = s->off_bphys + align256(sp::fused3::phys_bytes(n, fp64, rot));
+        cudaError_t e = sp::fused3::set_attributes(n, fp64, rot);
+        if (e != cudaSuccess) {
+            sp_destroy(s);
+            return set(SP_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+        }
+        if (status) *status = SP_OK;
+        return s;
+    }
     if (fft_mode == SP_FFT_FUSED) {
         s->kc = sp::fused::kc_of(n);
         size_t csz = 2 * s->rsize;
@@ -842,6 +906,11 @@ int sp_prepare(sp_solver* s, void* stream) {
         int r = upload_params(s, s->tab_valid ? s->tab_dt : 0.0, st);
         if (r) return r;
     }
+    if (s->fused3()) {
+        SP_CUDA(sp::fused3::mask(s->fp64, s->u0, s->n, st));
+        s->launches += 1;
+        return fused3_phase(s, 3, -1, st);
+    }
     if (s->fused()) {
         SP_CUDA(sp::fused::mask2d(s->fp64, s->u0, s->n, st));
         SP_CUDA(sp::fused::transpose_in(s->fp64, s->u0, s->u0t_dev(), s->n, s->kc, st));
@@ -904,7 +973,7 @@ int sp_step(sp_solver* s, double dt, void* stream) {
     auto st = (cudaStream_t)stream;
     int r = upload_params(s, dt, st);
     if (r) return r;
-    if (s->fused()) s->u0_fresh = false;
+    if (s->fused2()) s->u0_fresh = false;
     if (!s->graph_on) return run_step(s, st);
     if (!s->exec && (r = capture_step(s))) return r;
     SP_CUDA(cudaGraphLaunch(s->exec, st));
@@ -916,6 +985,12 @@ int sp_run_phase(sp_solver* s, int phase, int stage, void* stream) {
     SP_CHECK_BOUND(s);
     auto st = (cudaStream_t)stream;
     if (stage < 0 || stage > 3) return fail(s, SP_ERR_ARG, "sp_run_phase", "stage must be 0..3");
+    if (s->fused3()) {
+        if (phase < 0 || phase > 3) return fail(s, SP_ERR_ARG, "sp_run_phase", "phase must be 0..3");
+        if (phase == 3 && !s->params_valid)
+            return fail(s, SP_ERR_STATE, "sp_run_phase", "no step parameters yet");
+        return fused3_phase(s, phase, stage, st);
+    }
     if (s->fused()) {
         if (phase < 0 || phase > 3) return fail(s, SP_ERR_ARG, "sp_run_phase", "phase must be 0..3");
         if (phase == 0) return fused_row(s, st);
@@ -974,6 +1049,26 @@ int sp_max_velocity(sp_solver* s, const void* state, double* out_sum, double* ou
     if (!state || !out_sum) return fail(s, SP_ERR_ARG, "sp_max_velocity", "null pointer");
     auto st = (cudaStream_t)stream;
     int ncomp = s->dim;  // velocity components
+    if (s->fused3()) {
+        if (state != s->u0)
+            return fail(s, SP_ERR_UNSUPPORTED, "sp_max_velocity",
+                        "the fused engine bounds the velocity of its own state only");
+        SP_CUDA(cudaMemsetAsync(s->umax_dev(), 0, 4 * sizeof(unsigned long long), st));
+        int r = fused3_umax(s, st);
+        if (r) return r;
+        unsigned long long bits[4] = {0, 0, 0, 0};
+        SP_CUDA(cudaMemcpyAsync(bits, s->umax_dev(), sizeof(bits), cudaMemcpyDeviceToHost, st));
+        SP_CUDA(cudaStreamSynchronize(st));
+        double sum = 0.0;
+        for (int c = 0; c < 3; ++c) {
+            double v;
+            std::memcpy(&v, &bits[c], sizeof(v));
+            if (out_per_comp) out_per_comp[c] = v;
+            sum += v;
+        }
+        *out_sum = sum;
+        return SP_OK;
+    }
     if (s->fused()) {
         // the work array holds the stage-0 inputs of the live state: one inverse row pass
         if (state != s->u0)
@@ -1171,7 +1266,7 @@ int sp_run_to(sp_solver* s, double t_end, double cfl, double dt_max, int cfl_eve
     c.have_power = use_power ? 1 : 0;
     RunCtl* dc = (RunCtl*)((char*)s->aux + s->off_ctl);
     SP_CUDA(cudaMemcpyAsync(dc, &c, sizeof(RunCtl), cudaMemcpyHostToDevice, st));
-    if (s->fused()) s->u0_fresh = false;
+    if (s->fused2()) s->u0_fresh = false;
     int64_t chunks = 0;
     while (c.t < t_end - c.tol && c.steps < max_steps) {
         SP_CUDA(cudaGraphLaunch(s->run_exec, st));

@@ -59,8 +59,9 @@ REGISTRY: list[Variant] = [
             "as above, batched plans, whole step replayed from one CUDA graph with "
             "device-resident dt/forcing", default=True),
     Variant("b200", "fused-fft-graph", "solver", "B200FusedSolver", True,
-            "2D: hand-written sm_100a FFTs fused with every pointwise phase (row pass + column "
-            "pass per RK stage over the dealiased columns), no cuFFT, one CUDA graph per step"),
+            "hand-written sm_100a FFTs fused with every pointwise phase over the dealiased "
+            "modes (2D: row + column pass per RK stage; 3D: y, z, y and x passes), no cuFFT, "
+            "one CUDA graph per step"),
 ]
 
 

@@ -238,14 +238,18 @@ class B200LeanSolver(B200Solver):
 
 
 class B200FusedSolver(B200Solver):
-    """2D: hand-written FFTs fused with the pointwise phases — per RK stage one row pass
-    (inverse row FFT, products, forward row FFT) and one column pass (forward column FFT,
-    Lawson update, inverse column FFT) over the 2/3-dealiased columns; no cuFFT; one CUDA
-    graph per step.  n a power of two, 16..8192 (fp32) or 16..4096 (fp64)."""
+    """Hand-written FFTs fused with the pointwise phases, over the 2/3-dealiased modes only;
+    no cuFFT; one CUDA graph per step.
+
+    2D (Basdevant form; n a power of two, 16..8192 fp32 / 16..4096 fp64): per RK stage one row
+    pass (inverse row FFT, products, forward row FFT) and one column pass (forward column FFT,
+    Lawson update, inverse column FFT).  3D (Basdevant and rotational forms; n a power of two,
+    16..512): per RK stage a y-inverse pass, a z pass (c2r, products, r2c), a y-forward pass
+    and an x pass (forward FFT, Leray projection and Lawson update, inverse FFT)."""
 
     variant = "fused-fft-graph"
-    dims = (2,)
-    forms = ("basdevant",)
+    dims = (2, 3)
+    forms = ("basdevant", "rotational")
     fft_mode = _lib.FFT_FUSED
 
 
