@@ -410,11 +410,31 @@ def run_workload(s, w: dict, nsteps: int) -> None:
         run_steps(s, nsteps, cfl=w["cfl"], dt_max=0.05, cfl_every=10)
 
 
-def secondary_line(wname: str, steps: int, warmup: int, local: int) -> dict:
+def fused3d_pass_bytes(n: int, form: str, dtype: str) -> dict:
+    """Algorithmic bytes of one launch of each fused 3D pass at a middle RK stage: every
+    work-array element a pass reads or writes once (kept modes only), plus the compact state
+    and accumulator of the X pass (read the state and accumulator, write the accumulator)."""
+    sc = 16 if dtype == "float64" else 8  # one complex
+    pr = 2 * sc                           # one Pair (two kz columns)
+    km = (n - 1) // 3
+    kz, kk = km + 1, 2 * km + 1
+    nq = (kz + 1) // 2
+    nin, nfw = (6, 3) if form == "rotational" else (3, 5)
+    return {
+        "k3_yinv": n * nin * nq * (kk + n) * pr,
+        "k3_z": n * n * (nin + nfw) * kz * sc,
+        "k3_yfwd": n * nfw * nq * (n + kk) * pr,
+        "k3_x<stage 1>": kk * nq * (nfw + nin) * n * pr + 3 * 3 * kk * kz * kk * sc,
+    }
+
+
+def secondary_line(wname: str, steps: int, warmup: int, local: int,
+                   variant: str = "b200/fused-fft-graph") -> dict:
     """A second workload measured inside the same bench run (its own solver, CUDA-event time
     over ``steps`` steps after ``warmup``, its own clock samples): ms/step, Mpts/s, the
-    reference's FFT roofline, the roofline of its dominant own kernel and the error of one step
-    against the fp64 engine.  Used for the 512^3 3D Taylor-Green line beside the 2D headline."""
+    reference's FFT roofline, the roofline of the engine's dominant own kernel, the error of
+    one step against the fp64 cuFFT engine, and the cuFFT engine's own ms/step on the same
+    workload.  Used for the 512^3 3D Taylor-Green line beside the 2D headline."""
     import torch
 
     from pyspectral_b200.config import fft_split
@@ -423,41 +443,54 @@ def secondary_line(wname: str, steps: int, warmup: int, local: int) -> dict:
     w = WORKLOADS[wname]
     n, dim = w["n"], w["dim"]
     cfg = make_config(w)
-    variant = "b200/fused-inplace-graph"
-    s = make_solver(variant, cfg)
-    ic = tgv3d_device(n, torch.complex64) if w["ic"] == "tgv3d" else make_ic(w)
-    s.set_state(ic)
-    run_workload(s, w, warmup)
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    l0 = s.kernel_launches
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record()
-    run_workload(s, w, steps)
-    ev1.record()
-    ev1.synchronize()
-    clk = clocks.stop()
-    ms_step = ev0.elapsed_time(ev1) / steps
-    launches = s.kernel_launches - l0
+    fused = "fused-fft" in variant
 
-    def fft_stage() -> None:
-        s.run_phase(0)
-        s.run_phase(2)
+    def timed(v: str, with_clocks: bool):
+        sv = make_solver(v, cfg)
+        sv.set_state(tgv3d_device(n, torch.complex64) if w["ic"] == "tgv3d" else make_ic(w))
+        run_workload(sv, w, warmup)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local) if with_clocks else None
+        if clocks:
+            clocks.start()
+        l0 = sv.kernel_launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run_workload(sv, w, steps)
+        e1.record()
+        e1.synchronize()
+        clk = clocks.stop() if clocks else None
+        return sv, e0.elapsed_time(e1) / steps, sv.kernel_launches - l0, clk
 
-    t_fft_own = event_time_ms(fft_stage, 10)
-    t_fft_torch = torch_fft_stage_ms(w, *fft_split(dim, w["form"]))
-    t_fft = min(t_fft_own, t_fft_torch)
+    s, ms_step, launches, clk = timed(variant, True)
     tm = traffic_model(n, dim, w["form"], w["dtype"])
-    bcopy = copy_bandwidth_gbs()
-    t_roof = 4 * t_fft + tm["pointwise_bytes"] / (bcopy * 1e9) * 1e3
     sc = 16 if w["dtype"] == "float64" else 8
     ncomp = 1 if dim == 2 else 3
-    t_post = event_time_ms(lambda: s.run_phase(3, 1), 10)
-    post_bytes = (s.n_fwd + 2 * ncomp + ncomp + s.n_inv) * tm["modes"] * sc
+    if fused:
+        pb = fused3d_pass_bytes(n, w["form"], w["dtype"])
+        kernels = {name: (event_time_ms(lambda ph=ph: s.run_phase(ph, 1), 10), pb[name])
+                   for ph, name in enumerate(pb)}
+    else:
+        t_post = event_time_ms(lambda: s.run_phase(3, 1), 10)
+        post_bytes = (s.n_fwd + 2 * ncomp + ncomp + s.n_inv) * tm["modes"] * sc
+        kernels = {"k_post3d<stage 1>" if dim == 3 else "k_post2d<stage 1>": (t_post, post_bytes)}
+    # the reference's FFT ceiling: the cuFFT engine's standalone stage transforms
+    cf, cufft_ms, _, _ = (s, ms_step, 0, None) if not fused else timed("b200/fused-inplace-graph", False)
+
+    def fft_stage() -> None:
+        cf.run_phase(0)
+        cf.run_phase(2)
+
+    t_fft_own = event_time_ms(fft_stage, 10)
+    del cf
+    t_fft_torch = torch_fft_stage_ms(w, *fft_split(dim, w["form"]))
+    t_fft = min(t_fft_own, t_fft_torch)
+    bcopy = copy_bandwidth_gbs()
+    t_roof = 4 * t_fft + tm["pointwise_bytes"] / (bcopy * 1e9) * 1e3
     peak = measured_peaks().get("hbm_gbs")
-    achieved = post_bytes / (t_post * 1e-3) / 1e9
-    kname = "k_post2d<stage 1>" if dim == 2 else "k_post3d<stage 1>"
+    kname = max(kernels, key=lambda k: kernels[k][0])
+    k_ms, k_bytes = kernels[kname]
+    achieved = k_bytes / (k_ms * 1e-3) / 1e9
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
@@ -465,18 +498,19 @@ def secondary_line(wname: str, steps: int, warmup: int, local: int) -> dict:
             traffic = json.loads(tf.read_text()).get(wname, {}).get(kname)
         except Exception:  # noqa: BLE001
             traffic = None
-    # one step against the fp64 engine from the same state
+    # one step against the fp64 cuFFT engine from the same state
+    ic = tgv3d_device(n, torch.complex64) if w["ic"] == "tgv3d" else make_ic(w)
     s.set_state(ic)
     h = w.get("dt") or min(0.05, w["cfl"] * (2 * math.pi / n)
                            / s.diag.max_velocity_sum(s.state_native()))
     s.step(h)
     ua = s.state_native().clone()
-    del s
+    del s, ic
     gc.collect()
     torch.cuda.empty_cache()
     rel_err = None
     try:
-        b = make_solver(variant, cfg.with_(dtype="float64"))
+        b = make_solver("b200/fused-inplace-graph", cfg.with_(dtype="float64"))
         b.set_state(tgv3d_device(n, torch.complex128) if w["ic"] == "tgv3d" else make_ic(w))
         b.step(h)
         ub = b.state_native()
@@ -492,14 +526,16 @@ def secondary_line(wname: str, steps: int, warmup: int, local: int) -> dict:
         "dtype": "f32" if w["dtype"] == "float32" else "f64", "steps": steps, "warmup": warmup,
         "ms_per_step": ms_step, "value": float(n) ** dim / (ms_step * 1e-3) / 1e6,
         "unit": "Mpts/s", "pct_fft_roofline": 100.0 * t_roof / ms_step,
+        "cufft_engine_ms_per_step": cufft_ms,
         "fft_roofline": {"t_fft_stage_ms": t_fft, "t_fft_stage_ms_own_plans": t_fft_own,
                          "t_fft_stage_ms_torch_fft": t_fft_torch, "t_roofline_step_ms": t_roof,
                          "copy_bw_gbs": bcopy, "pointwise_bytes": tm["pointwise_bytes"]},
+        "own_kernels_ms": {k: v[0] for k, v in kernels.items()},
         "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
                      "peak": peak or FALLBACK_HBM_GBS, "unit": "GB/s",
                      "frac": achieved / (peak or FALLBACK_HBM_GBS),
                      "peak_source": "measured" if peak else "fallback",
-                     "algorithmic_bytes_per_launch": post_bytes, "traffic": traffic},
+                     "algorithmic_bytes_per_launch": k_bytes, "traffic": traffic},
         "rel_err_one_step_vs_fp64": rel_err, "gpu_launches": launches, "clocks": clk,
     }
 
@@ -947,7 +983,12 @@ def ours(args, w: dict) -> int:
     sc = 16 if w["dtype"] == "float64" else 8
     ncomp = 1 if w["dim"] == 2 else 3
     tm = traffic_model(w["n"], w["dim"], w["form"], w["dtype"])
-    if fused:
+    if fused and w["dim"] == 3:
+        pb = fused3d_pass_bytes(w["n"], w["form"], w["dtype"])
+        kernels = {name: (event_time_ms(lambda ph=ph: s.run_phase(ph, 1), 15), pb[name])
+                   for ph, name in enumerate(pb)}
+        del cf
+    elif fused:
         n = w["n"]
         kc = (n + 2) // 3
         kept_rows = 2 * ((n - 1) // 3) + 1
@@ -1045,8 +1086,9 @@ def main(argv: list[str] | None = None) -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="decay2d-8192-fp32", choices=sorted(WORKLOADS))
     ap.add_argument("--variant", default="auto",
-                    help="registry variant; auto = the fused-FFT engine where it runs (2D, n a "
-                         "power of two <= 8192 fp32 / 4096 fp64), else the cuFFT graph engine")
+                    help="registry variant; auto = the fused-FFT engine where it runs (n a "
+                         "power of two: 2D <= 8192 fp32 / 4096 fp64, 3D <= 512), else the "
+                         "cuFFT graph engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the 512^3 3D line measured beside the default 2D workload")
@@ -1093,8 +1135,9 @@ def main(argv: list[str] | None = None) -> int:
         return ours_big3d(args, w)
     if args.variant == "auto":
         n = w["n"]
-        fused_ok = (w["dim"] == 2 and n & (n - 1) == 0 and 16 <= n
-                    and n <= (8192 if w["dtype"] == "float32" else 4096))
+        pow2 = n & (n - 1) == 0 and 16 <= n
+        fused_ok = pow2 and (n <= (8192 if w["dtype"] == "float32" else 4096) if w["dim"] == 2
+                             else n <= 512)
         args.variant = "b200/fused-fft-graph" if fused_ok else "b200/fused-inplace-graph"
     if args.impl == "reference":
         return reference_arm(args, w)

@@ -188,6 +188,24 @@ cudaError_t x_pass(int n, int fp64, int rot, int stage, void* Bs, void* u0, void
     });
 }
 
+size_t compact_bytes(int n, int fp64) {
+    const size_t km = (size_t)(n - 1) / 3, kk = 2 * km + 1;
+    return 3 * kk * (km + 1) * kk * (fp64 ? 16 : 8);
+}
+
+cudaError_t state_move(int fp64, void* u0, void* compact, int n, int in, cudaStream_t st) {
+    const int km = (n - 1) / 3, kk = 2 * km + 1;
+    const dim3 grid((km + 1 + 31) / 32, (kk + 31) / 32, 3 * kk), block(32, 8);
+    if (fp64) {
+        if (in) f3::k3_state_move<double, true><<<grid, block, 0, st>>>((cplx<double>*)u0, (cplx<double>*)compact, n);
+        else f3::k3_state_move<double, false><<<grid, block, 0, st>>>((cplx<double>*)u0, (cplx<double>*)compact, n);
+    } else {
+        if (in) f3::k3_state_move<float, true><<<grid, block, 0, st>>>((cplx<float>*)u0, (cplx<float>*)compact, n);
+        else f3::k3_state_move<float, false><<<grid, block, 0, st>>>((cplx<float>*)u0, (cplx<float>*)compact, n);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t mask(int fp64, void* u0, int n, cudaStream_t st) {
     const int nh = n / 2 + 1;
     const uint32_t fsc = (uint32_t)n * (uint32_t)n * (uint32_t)nh;

@@ -11,15 +11,17 @@
 //   Y-forward : B_phys -> B_spec (forward along y, kept ky only, f < n_fwd)
 //   X         : per column (ky', kz pair): forward along x of the products, then for every
 //               kept kx the divergence / Leray projection / integrating factor / Lawson update
-//               of the state and accumulator (NumPy layout, updated in place) and the next
-//               stage's inputs, then inverse along x of those inputs; in place in B_spec
+//               of the state and accumulator and the next stage's inputs, then inverse along x
+//               of those inputs; in place in B_spec
 //
 // ky' and kx' index the kept wavenumbers -KM..KM (0..KM, then -KM..-1); kz is padded to an
 // even count so two adjacent kz columns move as one Pair (16 bytes in fp32): every 1D
 // transform of the Y and X passes is a Pair transform of two kz columns sharing twiddles.
 // Each transform is one warp's (n <= 512: n/16 threads, 16 elements per thread; several
-// transforms per warp below n = 512), and its exchanges are warp-synchronised.  The state u0
-// and the accumulator stay in the NumPy r2c layout, so diagnostics read the live state.
+// transforms per warp below n = 512), and its exchanges are warp-synchronised.  The state and
+// the accumulator live as compact copies of the kept modes, [c][ky'][kz][kx'] (kx' fastest, so
+// the X pass reads and writes them in whole rows); the NumPy-layout state u0 is refreshed from
+// the compact state only when it is read (k3_state_move).
 //
 // Equations (the reference's pre3d / phys3d_basd / phys3d_rot / post3d,
 // src/pyspectral/kernels/spectral.cu:164-238): Basdevant T = (uu - q, vv - q, uv, uw, vw),
@@ -392,6 +394,13 @@ struct XPass {
     static constexpr long UNITS = (long)D::KK * D::NQ;
 };
 
+// Index of kept mode (c, ky', kz, kx') in the compact state / accumulator.
+template <int N>
+__device__ __forceinline__ size_t compact_idx(int c, int kyi, int kz, int kxi) {
+    using D = Dims<N>;
+    return (((size_t)c * D::KK + kyi) * D::KZ + kz) * D::KK + kxi;
+}
+
 template <typename T, int N, bool ROT, int STAGE>
 __global__ void __launch_bounds__(XPass<N, ROT>::THREADS) k3_x(
     Pair<T>* __restrict__ Bs, cplx<T>* __restrict__ u0, cplx<T>* __restrict__ acc,
@@ -403,7 +412,6 @@ __global__ void __launch_bounds__(XPass<N, ROT>::THREADS) k3_x(
     constexpr int NIN = ninv<ROT>(), NFW = nfwd<ROT>();
     constexpr int RF0 = first_radix<N, false>(), RIL = last_radix<N, true>();
     constexpr int NH = N / 2 + 1;
-    constexpr size_t FSC = (size_t)N * N * NH;
     extern __shared__ __align__(16) unsigned char xsm[];
     Pair<T>* stage = reinterpret_cast<Pair<T>*>(xsm);  // [s][f][kx']
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -438,41 +446,38 @@ __global__ void __launch_bounds__(XPass<N, ROT>::THREADS) k3_x(
         __syncthreads();
     }
 
-    // every kept kx of the CTA's columns: update and next inputs
-    for (int e = threadIdx.x; e < S * KK; e += X::THREADS) {
-        const int s = e / KK, kxi = e % KK;
+    // every kept kx of the CTA's columns, one kz column at a time (kx' fastest: the compact
+    // state and accumulator rows are read and written contiguously): update and next inputs
+#pragma unroll 2
+    for (int e = threadIdx.x; e < S * 2 * KK; e += X::THREADS) {
+        const int kxi = e % KK, sh = e / KK, s = sh >> 1, h = sh & 1;
         const long us = (long)blockIdx.x * S + s;
         if (us >= X::UNITS) continue;
         const int qs = (int)(us % D::NQ), kyis = (int)(us / D::NQ);
-        const int kxs = kept_k<N>(kxi), kys = kept_k<N>(kyis);
-        const T kx = (T)kxs, ky = (T)kys;
-        const size_t row =
-            ((size_t)(kxs < 0 ? kxs + N : kxs) * N + (kys < 0 ? kys + N : kys)) * NH;
-        Pair<T> F[NFW];
-        if constexpr (STAGE >= 0) {
+        const int kzi = 2 * qs + h;
+        cplx<T> out[6];
 #pragma unroll
-            for (int f = 0; f < NFW; ++f) F[f] = st_at(s, f, kxi);
-        }
-        cplx<T> out[2][6];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int kzi = 2 * qs + h;
-#pragma unroll
-            for (int c = 0; c < 6; ++c) out[h][c] = mk<T>(0, 0);
-            if (kzi >= D::KZ) continue;  // the padding column
-            const T kz = (T)kzi, k2 = kx * kx + ky * ky + kz * kz;
-            const size_t o = row + kzi;
-            cplx<T> a = u0[o], b = u0[FSC + o], c = u0[2 * FSC + o];
+        for (int c = 0; c < 6; ++c) out[c] = mk<T>(0, 0);
+        if (kzi < D::KZ) {  // else the padding column: zero inputs
+            const int kxs = kept_k<N>(kxi), kys = kept_k<N>(kyis);
+            const T kx = (T)kxs, ky = (T)kys, kz = (T)kzi, k2 = kx * kx + ky * ky + kz * kz;
+            const size_t o = compact_idx<N>(0, kyis, kzi, kxi);
+            constexpr size_t CS = (size_t)D::KK * D::KZ * D::KK;  // one component
+            cplx<T> a = u0[o], b = u0[CS + o], c = u0[2 * CS + o];
             if constexpr (STAGE >= 0) {
+                cplx<T> F[NFW];
+#pragma unroll
+                for (int f = 0; f < NFW; ++f) {
+                    const Pair<T> pf = st_at(s, f, kxi);
+                    F[f] = h ? pf.b : pf.a;
+                }
                 cplx<T> N0, N1, N2;
                 if constexpr (ROT) {
-                    N0 = h ? F[0].b : F[0].a;
-                    N1 = h ? F[1].b : F[1].a;
-                    N2 = h ? F[2].b : F[2].a;
+                    N0 = F[0];
+                    N1 = F[1];
+                    N2 = F[2];
                 } else {
-                    const cplx<T> t11 = h ? F[0].b : F[0].a, t22 = h ? F[1].b : F[1].a,
-                                  t12 = h ? F[2].b : F[2].a, t13 = h ? F[3].b : F[3].a,
-                                  t23 = h ? F[4].b : F[4].a;
+                    const cplx<T> t11 = F[0], t22 = F[1], t12 = F[2], t13 = F[3], t23 = F[4];
                     const cplx<T> t33 = mk<T>(-(t11.x + t22.x), -(t11.y + t22.y));
                     N0 = mul_mi(add(add(scl(kx, t11), scl(ky, t12)), scl(kz, t13)));
                     N1 = mul_mi(add(add(scl(kx, t12), scl(ky, t22)), scl(kz, t23)));
@@ -487,20 +492,20 @@ __global__ void __launch_bounds__(XPass<N, ROT>::THREADS) k3_x(
                 const IFac<T> fac = if_factors(tab, NH, kxs < 0 ? -kxs : kxs,
                                                kys < 0 ? -kys : kys, kzi, k2, p);
                 cplx<T> Ca = STAGE > 0 ? acc[o] : mk<T>(0, 0);
-                cplx<T> Cb = STAGE > 0 ? acc[FSC + o] : mk<T>(0, 0);
-                cplx<T> Cc = STAGE > 0 ? acc[2 * FSC + o] : mk<T>(0, 0);
+                cplx<T> Cb = STAGE > 0 ? acc[CS + o] : mk<T>(0, 0);
+                cplx<T> Cc = STAGE > 0 ? acc[2 * CS + o] : mk<T>(0, 0);
                 constexpr int SG = STAGE < 0 ? 0 : STAGE;
                 a = lawson_stage<T, SG>(p.dt, fac, N0, a, Ca);
                 b = lawson_stage<T, SG>(p.dt, fac, N1, b, Cb);
                 c = lawson_stage<T, SG>(p.dt, fac, N2, c, Cc);
                 if (STAGE == 3) {
                     u0[o] = a;
-                    u0[FSC + o] = b;
-                    u0[2 * FSC + o] = c;
+                    u0[CS + o] = b;
+                    u0[2 * CS + o] = c;
                 } else {
                     acc[o] = Ca;
-                    acc[FSC + o] = Cb;
-                    acc[2 * FSC + o] = Cc;
+                    acc[CS + o] = Cb;
+                    acc[2 * CS + o] = Cc;
                 }
             }
             // next inputs: u scaled; rotational form also omega = i k x u
@@ -508,17 +513,21 @@ __global__ void __launch_bounds__(XPass<N, ROT>::THREADS) k3_x(
             a = scl(sc, a);
             b = scl(sc, b);
             c = scl(sc, c);
-            out[h][0] = a;
-            out[h][1] = b;
-            out[h][2] = c;
+            out[0] = a;
+            out[1] = b;
+            out[2] = c;
             if (ROT) {
-                out[h][3] = mul_i(add(scl(ky, c), scl(-kz, b)));
-                out[h][4] = mul_i(add(scl(kz, a), scl(-kx, c)));
-                out[h][5] = mul_i(add(scl(kx, b), scl(-ky, a)));
+                out[3] = mul_i(add(scl(ky, c), scl(-kz, b)));
+                out[4] = mul_i(add(scl(kz, a), scl(-kx, c)));
+                out[5] = mul_i(add(scl(kx, b), scl(-ky, a)));
             }
         }
 #pragma unroll
-        for (int c = 0; c < NIN; ++c) st_at(s, c, kxi) = Pair<T>{out[0][c], out[1][c]};
+        for (int c = 0; c < NIN; ++c) {
+            Pair<T>& slot = st_at(s, c, kxi);
+            if (h) slot.b = out[c];
+            else slot.a = out[c];
+        }
     }
     __syncthreads();
 
@@ -539,6 +548,47 @@ __global__ void __launch_bounds__(XPass<N, ROT>::THREADS) k3_x(
 #pragma unroll
                 for (int m = 0; m < RIL; ++m)
                     Bs[spec_idx<N, ROT>(in_pos<N, RIL>(t, g, m), f, kyi, q)] = v[g * RIL + m];
+        }
+    }
+}
+
+// Compact state <-> NumPy layout: for each (c, ky'), a [kx'][kz] slab of u0 (kz contiguous)
+// against the [kz][kx'] slab of the compact copy, through 32 x 33 shared tiles.  IN: u0 ->
+// compact; otherwise compact -> u0 (kept modes only; the others stay as they are, zero).
+template <typename T, bool IN>
+__global__ void __launch_bounds__(256) k3_state_move(cplx<T>* __restrict__ u0,
+                                                     cplx<T>* __restrict__ uc, int n) {
+    __shared__ cplx<T> tile[32][33];
+    const int km = (n - 1) / 3, kz_n = km + 1, kk = 2 * km + 1, nh = n / 2 + 1;
+    const int c = blockIdx.z / kk, kyi = blockIdx.z % kk;
+    const int ky = kyi <= km ? kyi : kyi - kk;
+    const size_t fsc = (size_t)n * n * nh;
+    cplx<T>* u = u0 + (size_t)c * fsc + (size_t)(ky < 0 ? ky + n : ky) * nh;  // + kx row * n nh
+    cplx<T>* w = uc + ((size_t)c * kk + kyi) * kz_n * kk;                      // [kz][kx']
+    const int x0 = blockIdx.y * 32, z0 = blockIdx.x * 32;
+    auto kx_row = [&](int kxi) -> size_t {
+        const int kx = kxi <= km ? kxi : kxi - kk;
+        return (size_t)(kx < 0 ? kx + n : kx) * n * nh;
+    };
+    if (IN) {
+        for (int r = threadIdx.y; r < 32; r += 8) {
+            const int kxi = x0 + r, kz = z0 + threadIdx.x;
+            if (kxi < kk && kz < kz_n) tile[r][threadIdx.x] = u[kx_row(kxi) + kz];
+        }
+        __syncthreads();
+        for (int r = threadIdx.y; r < 32; r += 8) {
+            const int kz = z0 + r, kxi = x0 + threadIdx.x;
+            if (kxi < kk && kz < kz_n) w[(size_t)kz * kk + kxi] = tile[threadIdx.x][r];
+        }
+    } else {
+        for (int r = threadIdx.y; r < 32; r += 8) {
+            const int kz = z0 + r, kxi = x0 + threadIdx.x;
+            if (kxi < kk && kz < kz_n) tile[r][threadIdx.x] = w[(size_t)kz * kk + kxi];
+        }
+        __syncthreads();
+        for (int r = threadIdx.y; r < 32; r += 8) {
+            const int kxi = x0 + r, kz = z0 + threadIdx.x;
+            if (kxi < kk && kz < kz_n) u[kx_row(kxi) + kz] = tile[threadIdx.x][r];
         }
     }
 }

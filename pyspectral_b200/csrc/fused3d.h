@@ -28,10 +28,15 @@ cudaError_t y_forward(int n, int fp64, int rot, const void* Bp, void* Bs, int nf
 // want_max: also record max |u_i| in mode 0.
 cudaError_t z_pass(int n, int fp64, int rot, int mode, void* Bp, const void* tw,
                    unsigned long long* umax, int want_max, cudaStream_t st);
-// X pass in place on B_spec with the state u0 and accumulator acc (NumPy layout, 3 fields
-// of n x n x (n/2+1)); stage -1 builds the stage-0 inputs from u0, 0..3 a Lawson stage.
+// X pass in place on B_spec with the compact state and accumulator; stage -1 builds the
+// stage-0 inputs from the state, 0..3 a Lawson stage.
 cudaError_t x_pass(int n, int fp64, int rot, int stage, void* Bs, void* u0, void* acc,
                    const void* tab, const void* params, const void* tw, cudaStream_t st);
+// Bytes of the compact state (and of the compact accumulator): the kept modes of the three
+// components, [c][ky'][kz][kx'].
+size_t compact_bytes(int n, int fp64);
+// Kept modes of the NumPy-layout state u0 into the compact copy (in != 0) or back.
+cudaError_t state_move(int fp64, void* u0, void* compact, int n, int in, cudaStream_t st);
 // Zero every mode outside the 2/3 mask of the three state components.
 cudaError_t mask(int fp64, void* u0, int n, cudaStream_t st);
 

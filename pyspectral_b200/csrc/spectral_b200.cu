@@ -87,7 +87,8 @@ struct sp_solver {
     // whether the NumPy-layout state u0 reflects the transposed state
     int kc = 0;
     size_t work_bytes = 0, off_u0t = 0;
-    // fused 3D mode: the work array is B_spec followed (at off_bphys) by B_phys
+    // fused 3D mode: the work array is B_spec, then (at off_bphys) B_phys, then (at off_u0t) the
+    // compact state; the compact accumulator lives at the start of acc
     size_t off_bphys = 0;
     bool u0_fresh = true;
     // cuFFT
@@ -383,7 +384,7 @@ int fused3_phase(sp_solver* s, int phase, int stage, cudaStream_t st) {
                                           s->tw_dev(), st));
             break;
         default:
-            SP_CUDA(sp::fused3::x_pass(s->n, s->fp64, s->rot(), stage, s->W, s->u0, s->acc,
+            SP_CUDA(sp::fused3::x_pass(s->n, s->fp64, s->rot(), stage, s->W, s->u0t_dev(), s->acc,
                                        s->tab_dev(), s->params_dev(), s->tw_dev(), st));
     }
     s->launches += 1;
@@ -766,7 +767,8 @@ sp_solver* sp_create(int n, int dim, int form, int fp64, int fft_mode, int* stat
     if (fft_mode == SP_FFT_FUSED && dim == 3) {
         const int rot = form == SP_FORM_ROTATIONAL ? 1 : 0;
         s->off_bphys = align256(sp::fused3::spec_bytes(n, fp64, rot));
-        s->work_bytes = s->off_bphys + align256(sp::fused3::phys_bytes(n, fp64, rot));
+        s->off_u0t = s->off_bphys + align256(sp::fused3::phys_bytes(n, fp64, rot));
+        s->work_bytes = s->off_u0t + align256(sp::fused3::compact_bytes(n, fp64));
         cudaError_t e = sp::fused3::set_attributes(n, fp64, rot);
         if (e != cudaSuccess) {
             sp_destroy(s);
@@ -908,7 +910,9 @@ int sp_prepare(sp_solver* s, void* stream) {
     }
     if (s->fused3()) {
         SP_CUDA(sp::fused3::mask(s->fp64, s->u0, s->n, st));
-        s->launches += 1;
+        SP_CUDA(sp::fused3::state_move(s->fp64, s->u0, s->u0t_dev(), s->n, 1, st));
+        s->launches += 2;
+        s->u0_fresh = true;
         return fused3_phase(s, 3, -1, st);
     }
     if (s->fused()) {
@@ -925,6 +929,12 @@ int sp_prepare(sp_solver* s, void* stream) {
 int sp_sync_state(sp_solver* s, void* stream) {
     SP_CHECK_BOUND(s);
     if (!s->fused() || s->u0_fresh) return SP_OK;
+    if (s->fused3()) {
+        SP_CUDA(sp::fused3::state_move(s->fp64, s->u0, s->u0t_dev(), s->n, 0, (cudaStream_t)stream));
+        s->launches += 1;
+        s->u0_fresh = true;
+        return SP_OK;
+    }
     SP_CUDA(sp::fused::transpose_out(s->fp64, s->u0t_dev(), s->u0, s->n, s->kc,
                                      (cudaStream_t)stream));
     s->launches += 1;
@@ -973,7 +983,7 @@ int sp_step(sp_solver* s, double dt, void* stream) {
     auto st = (cudaStream_t)stream;
     int r = upload_params(s, dt, st);
     if (r) return r;
-    if (s->fused2()) s->u0_fresh = false;
+    if (s->fused()) s->u0_fresh = false;
     if (!s->graph_on) return run_step(s, st);
     if (!s->exec && (r = capture_step(s))) return r;
     SP_CUDA(cudaGraphLaunch(s->exec, st));
@@ -989,6 +999,7 @@ int sp_run_phase(sp_solver* s, int phase, int stage, void* stream) {
         if (phase < 0 || phase > 3) return fail(s, SP_ERR_ARG, "sp_run_phase", "phase must be 0..3");
         if (phase == 3 && !s->params_valid)
             return fail(s, SP_ERR_STATE, "sp_run_phase", "no step parameters yet");
+        if (phase == 3) s->u0_fresh = false;
         return fused3_phase(s, phase, stage, st);
     }
     if (s->fused()) {
@@ -1266,7 +1277,7 @@ int sp_run_to(sp_solver* s, double t_end, double cfl, double dt_max, int cfl_eve
     c.have_power = use_power ? 1 : 0;
     RunCtl* dc = (RunCtl*)((char*)s->aux + s->off_ctl);
     SP_CUDA(cudaMemcpyAsync(dc, &c, sizeof(RunCtl), cudaMemcpyHostToDevice, st));
-    if (s->fused2()) s->u0_fresh = false;
+    if (s->fused()) s->u0_fresh = false;
     int64_t chunks = 0;
     while (c.t < t_end - c.tol && c.steps < max_steps) {
         SP_CUDA(cudaGraphLaunch(s->run_exec, st));
