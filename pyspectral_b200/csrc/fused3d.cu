@@ -23,8 +23,8 @@ constexpr size_t phys_pairs() {
 
 template <typename T, int N, bool ROT>
 cudaError_t attrs() {
-    using X = f3::XPass<N, ROT>;
-    const int smem = (int)X::template smem_bytes<T>();
+    using X = f3::XPass<T, N, ROT>;
+    const int smem = (int)X::smem_bytes();
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(f3::k3_x<T, N, ROT, -1>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem)))
@@ -45,10 +45,10 @@ cudaError_t attrs() {
 template <typename T, int N, bool ROT>
 cudaError_t yinv(const void* Bs, void* Bp, int nfields, const void* tw, cudaStream_t st) {
     using D = f3::Dims<N>;
-    constexpr int per = f3::kPassThreads / D::T;
+    constexpr int per = f3::y_threads<T>() / D::T;
     const long units = (long)N * nfields * D::NQ;
     const unsigned grid = (unsigned)((units + per - 1) / per);
-    f3::k3_yinv<T, N, ROT><<<grid, f3::kPassThreads, 0, st>>>(
+    f3::k3_yinv<T, N, ROT><<<grid, f3::y_threads<T>(), 0, st>>>(
         (const Pair<T>*)Bs, (Pair<T>*)Bp, nfields, (const cplx<T>*)tw);
     return cudaGetLastError();
 }
@@ -56,10 +56,10 @@ cudaError_t yinv(const void* Bs, void* Bp, int nfields, const void* tw, cudaStre
 template <typename T, int N, bool ROT>
 cudaError_t yfwd(const void* Bp, void* Bs, int nfields, const void* tw, cudaStream_t st) {
     using D = f3::Dims<N>;
-    constexpr int per = f3::kPassThreads / D::T;
+    constexpr int per = f3::y_threads<T>() / D::T;
     const long units = (long)N * nfields * D::NQ;
     const unsigned grid = (unsigned)((units + per - 1) / per);
-    f3::k3_yfwd<T, N, ROT><<<grid, f3::kPassThreads, 0, st>>>(
+    f3::k3_yfwd<T, N, ROT><<<grid, f3::y_threads<T>(), 0, st>>>(
         (const Pair<T>*)Bp, (Pair<T>*)Bs, nfields, (const cplx<T>*)tw);
     return cudaGetLastError();
 }
@@ -83,9 +83,9 @@ cudaError_t zp(int mode, void* Bp, const void* tw, unsigned long long* umax, int
 template <typename T, int N, bool ROT, int STAGE>
 cudaError_t xs(void* Bs, void* u0, void* acc, const void* tab, const void* params,
                const void* tw, cudaStream_t st) {
-    using X = f3::XPass<N, ROT>;
-    const unsigned grid = (unsigned)((X::UNITS + X::S - 1) / X::S);
-    f3::k3_x<T, N, ROT, STAGE><<<grid, X::THREADS, X::template smem_bytes<T>(), st>>>(
+    using X = f3::XPass<T, N, ROT>;
+    const unsigned grid = (unsigned)((X::UNITS + X::U - 1) / X::U);
+    f3::k3_x<T, N, ROT, STAGE><<<grid, X::THREADS, X::smem_bytes(), st>>>(
         (Pair<T>*)Bs, (cplx<T>*)u0, (cplx<T>*)acc, (const T*)tab,
         (const StepParams<T>*)params, (const cplx<T>*)tw);
     return cudaGetLastError();

@@ -4,7 +4,7 @@
 // modes only (2KM+1)^2 (KM+1) are ever non-zero — about 30 %.  The stage runs as four passes,
 // each a sweep of 1D transforms along one axis with the pointwise work of that point fused in:
 //
-//   Y-inverse : B_spec[x][f][ky'][kz] -> B_phys[x][f][y][kz]   (inverse along y, f < n_inv)
+//   Y-inverse : B_spec -> B_phys   (inverse along y, f < n_inv)
 //   Z         : per line (x, y): c2r along z of the velocity (and vorticity) fields, the
 //               physical-space products (Basdevant stress / u x omega), r2c along z of the
 //               products, kept kz only; in place in B_phys
@@ -14,9 +14,14 @@
 //               of the state and accumulator and the next stage's inputs, then inverse along x
 //               of those inputs; in place in B_spec
 //
-// ky' and kx' index the kept wavenumbers -KM..KM (0..KM, then -KM..-1); kz is padded to an
-// even count so two adjacent kz columns move as one Pair (16 bytes in fp32): every 1D
-// transform of the Y and X passes is a Pair transform of two kz columns sharing twiddles.
+// ky' and kx' index the kept wavenumbers -KM..KM (0..KM, then -KM..-1); kz is padded to a
+// multiple of four so two adjacent kz columns move as one Pair (16 bytes in fp32) and the
+// pairs per row are even: every 1D transform of the Y and X passes is a Pair transform of two
+// kz columns sharing twiddles.  B_spec interleaves x in pairs innermost,
+// B_spec[x/2][f][ky'][q][x%2] (q = kz pair), and B_phys keeps whole z lines,
+// B_phys[x][f][y][q].  An X-pass CTA holds two adjacent kz pairs of one ky' (its lanes t, t+1
+// hold x, x+1): runs of 64 bytes of B_spec.  A Y-pass CTA holds (x, x+1) x two adjacent kz
+// pairs: runs of 64 bytes of B_spec and 32 of B_phys.
 // Each transform is one warp's (n <= 512: n/16 threads, 16 elements per thread; several
 // transforms per warp below n = 512), and its exchanges are warp-synchronised.  The state and
 // the accumulator live as compact copies of the kept modes, [c][ky'][kz][kx'] (kx' fastest, so
@@ -42,8 +47,8 @@ struct Dims {
     static constexpr int KM = (N - 1) / 3;     // largest kept |k| (3 |k| < n)
     static constexpr int KZ = KM + 1;          // kept kz: 0..KM
     static constexpr int KK = 2 * KM + 1;      // kept kx, ky: -KM..KM
-    static constexpr int KZP = (KZ + 1) & ~1;  // kz extent padded to whole pairs
-    static constexpr int NQ = KZP / 2;         // kz pairs per row
+    static constexpr int NQ = (KZ + 3) / 4 * 2;  // kz pairs per row (even)
+    static constexpr int KZP = 2 * NQ;            // kz extent, padded
     static constexpr int T = N / 16;           // threads per transform
     static constexpr int SEQ = T >= 32 ? 1 : 32 / T;  // transforms per warp
     static_assert(N >= 16 && N <= 512 && (N & (N - 1)) == 0, "n a power of two, 16..512");
@@ -118,17 +123,35 @@ __device__ __forceinline__ Pair<T> pzero() {
     return Pair<T>{mk<T>(0, 0), mk<T>(0, 0)};
 }
 
-// Work-array indices in Pair units (two kz columns): B_spec [x][f][ky'][q], B_phys [x][f][y][q].
+// Work-array indices in Pair units (two kz columns): B_spec [x/2][f][ky'][q][x%2],
+// B_phys [x][f][y][q].
 template <int N, bool ROT>
 __device__ __forceinline__ size_t spec_idx(int x, int f, int ky, int q) {
-    return (((size_t)x * nslot<ROT>() + f) * Dims<N>::KK + ky) * Dims<N>::NQ + q;
+    return (((((size_t)(x >> 1) * nslot<ROT>() + f) * Dims<N>::KK + ky) * Dims<N>::NQ + q) << 1) |
+           (size_t)(x & 1);
 }
 template <int N, bool ROT>
 __device__ __forceinline__ size_t phys_idx(int x, int f, int y, int q) {
     return (((size_t)x * nslot<ROT>() + f) * N + y) * Dims<N>::NQ + q;
 }
 
-constexpr int kPassThreads = 128;  // Y passes: 4 warps per CTA
+// Unit of a Y pass: (x, f, q) with x % 2 fastest, then q, f, x / 2 — the consecutive units of
+// one CTA are x, x+1 for adjacent kz pairs.
+struct YUnit {
+    int x, f, q;
+};
+template <int N>
+__device__ __forceinline__ YUnit y_unit(long unit, int nfields) {
+    const int xl = (int)(unit & 1);
+    const long rest = unit >> 1;
+    const int q = (int)(rest % Dims<N>::NQ);
+    const long r2 = rest / Dims<N>::NQ;
+    return YUnit{2 * (int)(r2 / nfields) + xl, (int)(r2 % nfields), q};
+}
+
+// Y passes: 4 warps per CTA (8 measured no faster at 512^3)
+template <typename T>
+constexpr int y_threads() { return 128; }
 // Z pass: 4 warps (fp32) or 2 (fp64), so its static shared memory stays below 48 KB
 template <typename T>
 constexpr int z_threads() { return sizeof(T) == 4 ? 128 : 64; }
@@ -136,20 +159,19 @@ constexpr int z_threads() { return sizeof(T) == 4 ? 128 : 64; }
 // ------------------------------------------------------------------------------- Y passes
 // Inverse along y of fields f < nfields: one Pair transform per (x, f, kz pair).
 template <typename T, int N, bool ROT>
-__global__ void __launch_bounds__(kPassThreads) k3_yinv(const Pair<T>* __restrict__ Bs,
+__global__ void __launch_bounds__(y_threads<T>()) k3_yinv(const Pair<T>* __restrict__ Bs,
                                                         Pair<T>* __restrict__ Bp, int nfields,
                                                         const cplx<T>* __restrict__ tw) {
     using D = Dims<N>;
     constexpr int TT = D::T;
     constexpr int RIL = last_radix<N, true>();
-    __shared__ __align__(16) cplx<T> exch[kPassThreads / TT][FftPlan<N>::SMEM];
+    __shared__ __align__(16) cplx<T> exch[y_threads<T>() / TT][FftPlan<N>::SMEM];
     const int seq = threadIdx.x / TT, t = threadIdx.x % TT;
     const long units = (long)N * nfields * D::NQ;
-    const long unit = (long)blockIdx.x * (kPassThreads / TT) + seq;
+    const long unit = (long)blockIdx.x * (y_threads<T>() / TT) + seq;
     const bool active = unit < units;
-    const int q = (int)(unit % D::NQ);
-    const long r = unit / D::NQ;
-    const int f = (int)(r % nfields), x = (int)(r / nfields);
+    const YUnit yu = y_unit<N>(unit, nfields);
+    const int x = yu.x, f = yu.f, q = yu.q;
     Pair<T> v[16];
     for_slots([&](auto mc) {
         constexpr int M = decltype(mc)::value;
@@ -169,20 +191,19 @@ __global__ void __launch_bounds__(kPassThreads) k3_yinv(const Pair<T>* __restric
 
 // Forward along y of fields f < nfields, kept ky only.
 template <typename T, int N, bool ROT>
-__global__ void __launch_bounds__(kPassThreads) k3_yfwd(const Pair<T>* __restrict__ Bp,
+__global__ void __launch_bounds__(y_threads<T>()) k3_yfwd(const Pair<T>* __restrict__ Bp,
                                                         Pair<T>* __restrict__ Bs, int nfields,
                                                         const cplx<T>* __restrict__ tw) {
     using D = Dims<N>;
     constexpr int TT = D::T;
     constexpr int RF0 = first_radix<N, false>();
-    __shared__ __align__(16) cplx<T> exch[kPassThreads / TT][FftPlan<N>::SMEM];
+    __shared__ __align__(16) cplx<T> exch[y_threads<T>() / TT][FftPlan<N>::SMEM];
     const int seq = threadIdx.x / TT, t = threadIdx.x % TT;
     const long units = (long)N * nfields * D::NQ;
-    const long unit = (long)blockIdx.x * (kPassThreads / TT) + seq;
+    const long unit = (long)blockIdx.x * (y_threads<T>() / TT) + seq;
     const bool active = unit < units;
-    const int q = (int)(unit % D::NQ);
-    const long r = unit / D::NQ;
-    const int f = (int)(r % nfields), x = (int)(r / nfields);
+    const YUnit yu = y_unit<N>(unit, nfields);
+    const int x = yu.x, f = yu.f, q = yu.q;
     Pair<T> v[16];
 #pragma unroll
     for (int g = 0; g < 16 / RF0; ++g)
@@ -228,7 +249,6 @@ __global__ void __launch_bounds__(z_threads<T>()) k3_z(Pair<T>* __restrict__ Bp,
     constexpr int TT = D::T;
     constexpr int ZT = z_threads<T>();
     constexpr int NS = ZT / TT;
-    constexpr int KZP = D::KZP;
     __shared__ __align__(16) cplx<T> exch[NS][FftPlan<N>::SMEM];
     // each thread's 16 points of (omega_y, omega_z) (rotational) or of v w (Basdevant), kept
     // in shared memory between the transforms (thread-private)
@@ -238,9 +258,9 @@ __global__ void __launch_bounds__(z_threads<T>()) k3_z(Pair<T>* __restrict__ Bp,
     const bool active = line < (long)N * N;
     const int x = (int)(line / N), y = (int)(line % N);
     cplx<T>* B = reinterpret_cast<cplx<T>*>(Bp);
-    // complex index of (x, f, y, kz)
+    // complex index of (x, f, y, kz): B_phys rows of whole z lines
     auto at = [&](int f, int kz) -> size_t {
-        return (((size_t)x * nslot<ROT>() + f) * N + y) * KZP + kz;
+        return (((size_t)x * nslot<ROT>() + f) * N + y) * D::KZP + kz;
     };
     cplx<T>* sm = exch[seq];
     const cplx<T> z0 = mk<T>(0, 0);
@@ -375,21 +395,23 @@ __global__ void __launch_bounds__(z_threads<T>()) k3_z(Pair<T>* __restrict__ Bp,
 }
 
 // ------------------------------------------------------------------------------- X pass
-// One CTA per group of kz-pair columns: field warps f (one warp per field slot), SEQ transforms
-// per warp (units (ky', q) = blockIdx.x * SEQ + s).  STAGE -1: the stage-0 inputs from the
-// state (no forward transform, no update).
-template <int N, bool ROT>
+// A CTA holds U units (ky', q) = blockIdx.x U + u: G groups of field warps (one warp per field
+// slot), each warp SEQ transforms.  U = 2 (two adjacent kz pairs) except in fp64 at n = 512,
+// where the shared memory holds one.  STAGE -1: the stage-0 inputs from the state (no forward
+// transform, no update).
+template <typename T, int N, bool ROT>
 struct XPass {
     using D = Dims<N>;
-    static constexpr int THREADS = nslot<ROT>() * 32;
     static constexpr int S = D::SEQ;
-    template <typename T>
+    static constexpr int G = (S >= 2 || sizeof(T) == 8) ? 1 : 2;
+    static constexpr int U = G * S;
+    static constexpr int WARPS = G * nslot<ROT>();
+    static constexpr int THREADS = WARPS * 32;
     static constexpr size_t stage_bytes() {
-        return (size_t)S * nslot<ROT>() * D::KK * sizeof(Pair<T>);
+        return (size_t)U * nslot<ROT>() * D::KK * sizeof(Pair<T>);
     }
-    template <typename T>
     static constexpr size_t smem_bytes() {
-        return stage_bytes<T>() + (size_t)nslot<ROT>() * S * FftPlan<N>::SMEM * sizeof(cplx<T>);
+        return stage_bytes() + (size_t)WARPS * S * FftPlan<N>::SMEM * sizeof(cplx<T>);
     }
     static constexpr long UNITS = (long)D::KK * D::NQ;
 };
@@ -402,23 +424,24 @@ __device__ __forceinline__ size_t compact_idx(int c, int kyi, int kz, int kxi) {
 }
 
 template <typename T, int N, bool ROT, int STAGE>
-__global__ void __launch_bounds__(XPass<N, ROT>::THREADS) k3_x(
+__global__ void __launch_bounds__(XPass<T, N, ROT>::THREADS, 2) k3_x(
     Pair<T>* __restrict__ Bs, cplx<T>* __restrict__ u0, cplx<T>* __restrict__ acc,
     const T* __restrict__ tab, const StepParams<T>* __restrict__ P,
     const cplx<T>* __restrict__ tw) {
     using D = Dims<N>;
-    using X = XPass<N, ROT>;
-    constexpr int TT = D::T, S = X::S, KK = D::KK, NF = nslot<ROT>();
+    using X = XPass<T, N, ROT>;
+    constexpr int TT = D::T, S = X::S, U = X::U, KK = D::KK, NF = nslot<ROT>();
     constexpr int NIN = ninv<ROT>(), NFW = nfwd<ROT>();
     constexpr int RF0 = first_radix<N, false>(), RIL = last_radix<N, true>();
     constexpr int NH = N / 2 + 1;
     extern __shared__ __align__(16) unsigned char xsm[];
-    Pair<T>* stage = reinterpret_cast<Pair<T>*>(xsm);  // [s][f][kx']
+    Pair<T>* stage = reinterpret_cast<Pair<T>*>(xsm);  // [u][f][kx']
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int sub = lane / TT, t = lane % TT;
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(xsm + X::template stage_bytes<T>()) +
-                  (size_t)(warp * S + sub) * FftPlan<N>::SMEM;
-    const long unit = (long)blockIdx.x * S + sub;
+    const int fw = warp % NF;                               // this warp's field slot
+    const int sub = (warp / NF) * S + lane / TT, t = lane % TT;  // this sequence's unit in the CTA
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(xsm + X::stage_bytes()) +
+                  (size_t)(warp * S + lane / TT) * FftPlan<N>::SMEM;
+    const long unit = (long)blockIdx.x * U + sub;
     const bool active = unit < X::UNITS;
     const int q = (int)(unit % D::NQ), kyi = (int)(unit / D::NQ);
     const StepParams<T> p = *P;
@@ -428,8 +451,8 @@ __global__ void __launch_bounds__(XPass<N, ROT>::THREADS) k3_x(
 
     // forward along x of the products, kept kx into the staging buffer
     if constexpr (STAGE >= 0) {
-        if (warp < NFW) {
-            const int f = warp;
+        if (fw < NFW) {
+            const int f = fw;
             Pair<T> v[16];
 #pragma unroll
             for (int g = 0; g < 16 / RF0; ++g)
@@ -449,9 +472,9 @@ __global__ void __launch_bounds__(XPass<N, ROT>::THREADS) k3_x(
     // every kept kx of the CTA's columns, one kz column at a time (kx' fastest: the compact
     // state and accumulator rows are read and written contiguously): update and next inputs
 #pragma unroll 2
-    for (int e = threadIdx.x; e < S * 2 * KK; e += X::THREADS) {
+    for (int e = threadIdx.x; e < U * 2 * KK; e += X::THREADS) {
         const int kxi = e % KK, sh = e / KK, s = sh >> 1, h = sh & 1;
-        const long us = (long)blockIdx.x * S + s;
+        const long us = (long)blockIdx.x * U + s;
         if (us >= X::UNITS) continue;
         const int qs = (int)(us % D::NQ), kyis = (int)(us / D::NQ);
         const int kzi = 2 * qs + h;
@@ -532,8 +555,8 @@ __global__ void __launch_bounds__(XPass<N, ROT>::THREADS) k3_x(
     __syncthreads();
 
     // inverse along x of the next inputs
-    if (warp < NIN) {
-        const int f = warp;
+    if (fw < NIN) {
+        const int f = fw;
         Pair<T> v[16];
         for_slots([&](auto mc) {
             constexpr int M = decltype(mc)::value;

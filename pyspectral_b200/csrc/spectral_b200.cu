@@ -602,6 +602,11 @@ int enqueue_run_diag(sp_solver* s, bool need_umax, bool need_band, cudaStream_t 
         }
     }
     if (need_band) {
+        if (s->fused3()) {
+            // the live state is the compact copy: refresh the NumPy-layout state it sums over
+            SP_CUDA(sp::fused3::state_move(s->fp64, s->u0, s->u0t_dev(), s->n, 0, st));
+            s->launches += 1;
+        }
         if (s->fused2()) {
             SP_CUDA(sp::fused::reduce_t(s->fp64, s->u0t_dev(), s->n, s->kc, 0, 1, s->klo, s->khi,
                                         s->partials_dev(), kRedBlocks, s->out_dev(), st));
