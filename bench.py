@@ -418,7 +418,7 @@ def fused3d_pass_bytes(n: int, form: str, dtype: str) -> dict:
     pr = 2 * sc                           # one Pair (two kz columns)
     km = (n - 1) // 3
     kz, kk = km + 1, 2 * km + 1
-    nq = (kz + 1) // 2
+    nq = (kz + 3) // 4 * 2  # kz pairs per row, padded to an even count
     nin, nfw = (6, 3) if form == "rotational" else (3, 5)
     return {
         "k3_yinv": n * nin * nq * (kk + n) * pr,
