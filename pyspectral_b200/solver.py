@@ -127,8 +127,8 @@ class B200Solver(SpectralSolver):
 
         Same contract as check_state + set_state of the reference (shape ValueError, 2/3 mask),
         with the mask applied on the device by the engine's load kernel: the host only casts
-        into a pinned staging buffer (torch's threaded copy), the copy to the device is
-        asynchronous.
+        into a pinned staging buffer (torch's threaded copy) and the copy to the device is
+        asynchronous, chunk by chunk, so a chunk crosses PCIe while the next one is cast.
         """
         torch = self.torch
         if isinstance(state_hat, torch.Tensor) and state_hat.is_cuda:
@@ -145,10 +145,22 @@ class B200Solver(SpectralSolver):
             # torch's CPU copy casts with all host threads (numpy's copyto casts on one)
             if a.dtype not in (np.complex64, np.complex128, np.float32, np.float64):
                 a = a.astype(np.complex128)
-            stage.copy_(torch.from_numpy(np.ascontiguousarray(a)))
-            self.u0.copy_(stage, non_blocking=True)
+            src = torch.from_numpy(np.ascontiguousarray(a)).view(-1)
+            sflat, dflat = stage.view(-1), self.u0.view(-1)
+            for lo, hi in self._chunks(sflat.numel()):
+                sflat[lo:hi].copy_(src[lo:hi])
+                dflat[lo:hi].copy_(sflat[lo:hi], non_blocking=True)
             self._staging_free.record(torch.cuda.current_stream(self.device))
         self._check(self.lib.sp_prepare(self._h, self._stream()), "sp_prepare")
+
+    @staticmethod
+    def _chunks(count: int, parts: int = 8) -> list[tuple[int, int]]:
+        """[lo, hi) element ranges of a state split for host/PCIe overlap (states of a few
+        MB move whole)."""
+        if count < (1 << 21):
+            return [(0, count)]
+        step = -(-count // parts)
+        return [(lo, min(count, lo + step)) for lo in range(0, count, step)]
 
     def _host_staging(self) -> Any:
         """Pinned host buffer of the state's shape and dtype (reused; waits for its last copy)."""
@@ -161,15 +173,26 @@ class B200Solver(SpectralSolver):
         return self._staging
 
     def get_state(self) -> np.ndarray:
-        """The state copied to the host as complex128 (through the pinned staging buffer; the
-        widening cast runs on all host threads)."""
+        """The state copied to the host as complex128 (through the pinned staging buffer, chunk
+        by chunk: the widening cast of a chunk, on all host threads, overlaps the copy of the
+        next one over PCIe)."""
         torch = self.torch
         stage = self._host_staging()
-        stage.copy_(self.state_native(), non_blocking=True)
-        torch.cuda.current_stream(self.device).synchronize()
-        _lib.check_device_errors(self.lib)
+        src, sflat = self.state_native().view(-1), stage.view(-1)
+        stream = torch.cuda.current_stream(self.device)
+        chunks = self._chunks(sflat.numel())
+        landed = []
+        for lo, hi in chunks:
+            sflat[lo:hi].copy_(src[lo:hi], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            landed.append(ev)
         out = torch.empty(stage.shape, dtype=torch.complex128)
-        out.copy_(stage)
+        oflat = out.view(-1)
+        for (lo, hi), ev in zip(chunks, landed):
+            ev.synchronize()
+            oflat[lo:hi].copy_(sflat[lo:hi])
+        _lib.check_device_errors(self.lib)
         return out.numpy()
 
     def state_native(self) -> Any:

@@ -5,7 +5,8 @@ The reference validates this flow by its dissipation eps(t) = 2 nu Z(t)
 (src/pyspectral/validation.py:152-200).  tests/golden/tgv3d_re1600_n128_fp64.json is the
 oracle's run (tests/golden/make_tgv3d_oracle.py: rotational form, CFL 0.5, dt_max 0.05, dt
 refreshed every 10 steps, records every 0.1); the device runs the same schedule through
-``simulate.run``.  fp64: every record's energy and enstrophy within 1e-9 relative, and the
+``simulate.run`` on both 3D engines (cuFFT, and the fused passes of this library).  fp64: every
+record's energy and enstrophy within 1e-9 relative, and the
 same number of steps; the Basdevant form reaches the same flow (the two forms differ by a
 gradient that the projection removes).  fp32: the dissipation history within 1e-3 of the peak.
 """
@@ -26,9 +27,13 @@ FIX = json.loads((Path(__file__).parent / "golden" / "tgv3d_re1600_n128_fp64.jso
 REF = {"t": FIX["t"], "dissipation": [2.0 * TGV_NU * z for z in FIX["enstrophy"]]}
 
 
+ENGINES = ["b200/fused-inplace-graph", "b200/fused-fft-graph"]  # cuFFT, hand-written passes
+
+
+@pytest.mark.parametrize("variant", ENGINES)
 @pytest.mark.parametrize("form", ["rotational", "basdevant"])
-def test_tgv3d_128_fp64_matches_the_oracle_to_t10(form):
-    r = tgv3d("b200/fused-inplace-graph", FIX["n"], FIX["t_end"], cfl=FIX["cfl"],
+def test_tgv3d_128_fp64_matches_the_oracle_to_t10(form, variant):
+    r = tgv3d(variant, FIX["n"], FIX["t_end"], cfl=FIX["cfl"],
               dtype="float64", diag_dt=FIX["diag_dt"], form=form)
     assert r["steps"] == FIX["steps"]
     assert np.allclose(r["t"], FIX["t"], rtol=0, atol=1e-12)
@@ -37,8 +42,9 @@ def test_tgv3d_128_fp64_matches_the_oracle_to_t10(form):
         assert np.abs(a / b - 1).max() < 1e-9, key
 
 
-def test_tgv3d_128_fp32_dissipation_follows_the_oracle():
-    r = tgv3d("b200/fused-inplace-graph", FIX["n"], FIX["t_end"], cfl=FIX["cfl"],
+@pytest.mark.parametrize("variant", ENGINES)
+def test_tgv3d_128_fp32_dissipation_follows_the_oracle(variant):
+    r = tgv3d(variant, FIX["n"], FIX["t_end"], cfl=FIX["cfl"],
               dtype="float32", diag_dt=FIX["diag_dt"], form="rotational")
     c = compare_dissipation(np.array(r["t"]), np.array(r["dissipation_2nuZ"]), REF)
     assert c["max_abs_err_over_peak"] < 1e-3
