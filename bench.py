@@ -724,7 +724,10 @@ def ours_ensemble(args, w: dict) -> int:
                    "forcing": f"constant power P={w['power']} on {w['klo']}<=|k|<={w['khi']}",
                    "drag": f"alpha={w['alpha']} on |k|<={w['alpha_kmax']}",
                    "nu": "k_max eta = 1 (nu_for_kmax_eta)", "cfl": w["cfl"],
-                   "engine": "sp_batch per size class, one sp_group graph",
+                   "engine": ("work list: per RK stage one persistent row-pass and one "
+                              f"column-pass launch over every class, {ens.worklist}-thread CTAs"
+                              if ens is not None and ens.worklist else
+                              "sp_batch per size class, one sp_group graph (a branch per class)"),
                    "tiles": {str(c.n): c.tile for c in ens.classes} if ens is not None else {},
                    "tile_source": "TileTuner (CUDA-event timing of each candidate, JSON cache)"
                    if ens is not None and ens.tuner is not None else "default",
@@ -739,8 +742,7 @@ def ours_ensemble(args, w: dict) -> int:
                 "what": "set_states(host) + K steps + get_state of every member, wall clock"},
         "gpu_launches": launches, "clocks": clk,
         "autotune": None if ens is None or ens.tuner is None else {
-            k: {"tile": v["tile"], "ms_per_step": v["ms_per_step"], "cached": v["cached"]}
-            for k, v in ens.tuner.report.items()},
+            k: dict(v) for k, v in ens.tuner.report.items()},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = time_oracle_ensemble(w)

@@ -236,11 +236,27 @@ int sp_batch_diagnostics(sp_batch* b, double band_klo, double band_khi, double* 
 int sp_batch_max_velocity(sp_batch* b, double* out, void* stream);
 int64_t sp_batch_kernel_launches(const sp_batch* b);
 const char* sp_batch_last_error(const sp_batch* b);
-/* A group of bound, prepared batches stepped together from one graph (one branch each). */
+/* A group of bound, prepared batches stepped together from one graph: by default one branch
+ * per batch (one launch per batch and phase); with a work list, one persistent launch per
+ * phase over every batch.  No counterpart in the reference. */
 sp_group* sp_group_create(sp_batch** batches, int count, int* status);
 void sp_group_destroy(sp_group* g);
 int sp_group_step(sp_group* g, void* stream);
 const char* sp_group_last_error(const sp_group* g);
+/* Work list: the group's row and column passes as two persistent launches per RK stage that
+ * take packed items (class, member, 16 mt / n rows or columns) of every batch, CTAs of mt = 64
+ * or 128 threads.  Runs batches of one precision with n a power of two, n / 16 <= mt and
+ * 16 mt / n <= n (mt 64: n = 32..1024; 128: 64..1024); each item runs the single-run passes'
+ * code.  *bytes = the device buffer the lists need (0 when no mt applies); sp_group_bind takes
+ * a caller-owned buffer of that size (256-byte aligned); sp_group_set_worklist(g, mt) builds
+ * and uploads the lists (synchronous; the batches must be bound; 0 returns to one launch per
+ * batch) and drops the group's graph. */
+int sp_group_worklist_bytes(const sp_group* g, int64_t* bytes);
+int sp_group_bind(sp_group* g, void* buffer);
+int sp_group_set_worklist(sp_group* g, int mt);
+int sp_group_worklist(const sp_group* g);
+/* Kernels the work-list group steps launched (the per-batch counters count the other path). */
+int64_t sp_group_kernel_launches(const sp_group* g);
 
 /* ---------------------------------------------------------------- tensor-core tiles
  * Check of the BF16 tcgen05 tile path the closure network uses (no reference counterpart):

@@ -74,6 +74,11 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "sp_group_destroy": (None, [_vp]),
     "sp_group_step": (_i, [_vp, _vp]),
     "sp_group_last_error": (ctypes.c_char_p, [_vp]),
+    "sp_group_worklist_bytes": (_i, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "sp_group_bind": (_i, [_vp, _vp]),
+    "sp_group_set_worklist": (_i, [_vp, _i]),
+    "sp_group_worklist": (_i, [_vp]),
+    "sp_group_kernel_launches": (ctypes.c_int64, [_vp]),
     "sp_mma_tile_check": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _vp]),
     "sp_nonlinear": (_i, [_vp, _vp, _vp, _vp]),
     "sp_filter_spectrum": (_i, [_vp, _i, _vp, _i, _i, _i, _i, _vp]),

@@ -59,6 +59,12 @@ struct sp_group {
     std::vector<cudaEvent_t> events;
     cudaStream_t cap = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // work list (sp_group_bind, sp_group_set_worklist): class descriptors, row items and
+    // column items in the caller's device buffer; mt = 0: one launch per class and phase
+    void* wl = nullptr;
+    int mt = 0, nrow = 0, ncol = 0;
+    size_t off_rows = 0, off_cols = 0;
+    int64_t launches = 0;
     std::string err;
 };
 
@@ -111,6 +117,61 @@ int batch_step_kernels(sp_batch* b, cudaStream_t st) {
                                       b->base(b->off_tw), st, b->members, xs, us,
                                       b->tab_stride, b->tile));
         b->launches += 2;
+    }
+    return SP_OK;
+}
+
+// The work lists of a group for CTAs of mt threads: per class its descriptor, then per member
+// its rows and its kept columns in items of 16 mt / n.
+void group_lists(const sp_group* g, int mt, std::vector<sp::fused::MultiClass>& cls,
+                 std::vector<sp::fused::MultiItem>& rows, std::vector<sp::fused::MultiItem>& cols) {
+    cls.clear();
+    rows.clear();
+    cols.clear();
+    for (size_t ci = 0; ci < g->batches.size(); ++ci) {
+        const sp_batch* b = g->batches[ci];
+        sp::fused::MultiClass c{};
+        c.X = b->W;
+        c.u0t = (char*)b->W + b->off_u0t;
+        c.acct = (char*)b->W + b->off_acct;
+        c.tab = b->base(b->off_tab);
+        c.params = b->base(b->off_params);
+        c.tw = b->base(b->off_tw);
+        c.x_stride = b->member_work / b->psize;
+        c.u_stride = b->member_work / b->csize;
+        c.tab_stride = b->tab_stride;
+        c.n = b->n;
+        c.kc = b->kc;
+        cls.push_back(c);
+        const int per = sp::fused::multi_per_item(b->n, mt);
+        for (int m = 0; m < b->members; ++m) {
+            for (int r = 0; r < b->n; r += per) rows.push_back({(int)ci, m, r});
+            for (int k = 0; k < b->kc; k += per) cols.push_back({(int)ci, m, k});
+        }
+    }
+}
+
+bool group_multi_ok(const sp_group* g, int mt) {
+    for (const sp_batch* b : g->batches)
+        if (b->fp64 != g->batches[0]->fp64 || !sp::fused::multi_supported(b->n, mt)) return false;
+    return true;
+}
+
+size_t list_bytes(size_t ncls, size_t nrow, size_t ncol) {
+    return al256(ncls * sizeof(sp::fused::MultiClass)) +
+           al256(nrow * sizeof(sp::fused::MultiItem)) + ncol * sizeof(sp::fused::MultiItem);
+}
+
+int group_step_multi(sp_group* g, cudaStream_t st) {
+    const int fp64 = g->batches[0]->fp64;
+    const char* base = (const char*)g->wl;
+    cudaError_t e;
+    for (int stage = 0; stage < 4; ++stage) {
+        if ((e = sp::fused::row_multi(fp64, g->mt, base, base + g->off_rows, g->nrow, st)) ||
+            (e = sp::fused::col_multi(fp64, g->mt, stage, base, base + g->off_cols, g->ncol, st))) {
+            g->err = std::string("work-list pass: ") + cudaGetErrorString(e);
+            return SP_ERR_CUDA;
+        }
     }
     return SP_OK;
 }
@@ -418,20 +479,25 @@ int sp_group_step(sp_group* g, void* stream) {
         if ((e = cudaStreamBeginCapture(g->cap, cudaStreamCaptureModeThreadLocal)))
             return gfail("cudaStreamBeginCapture", e);
         int r = SP_OK;
-        cudaEventRecord(g->events[nb], g->cap);
-        for (size_t i = 0; i < nb && !r; ++i) {
-            cudaStreamWaitEvent(g->streams[i], g->events[nb], 0);
-            const int64_t before = g->batches[i]->launches;
-            r = batch_step_kernels(g->batches[i], g->streams[i]);
-            g->batches[i]->launches = before;
-            cudaEventRecord(g->events[i], g->streams[i]);
-            cudaStreamWaitEvent(g->cap, g->events[i], 0);
+        if (g->mt > 0) {
+            // one launch per phase over the packed work list of every class
+            r = group_step_multi(g, g->cap);
+        } else {
+            cudaEventRecord(g->events[nb], g->cap);
+            for (size_t i = 0; i < nb && !r; ++i) {
+                cudaStreamWaitEvent(g->streams[i], g->events[nb], 0);
+                const int64_t before = g->batches[i]->launches;
+                r = batch_step_kernels(g->batches[i], g->streams[i]);
+                g->batches[i]->launches = before;
+                cudaEventRecord(g->events[i], g->streams[i]);
+                cudaStreamWaitEvent(g->cap, g->events[i], 0);
+            }
         }
         cudaGraph_t graph = nullptr;
         e = cudaStreamEndCapture(g->cap, &graph);
         if (r) {
             if (graph) cudaGraphDestroy(graph);
-            g->err = "capture failed: " + g->batches[0]->err;
+            if (g->mt == 0) g->err = "capture failed: " + g->batches[0]->err;
             return r;
         }
         if (e != cudaSuccess) return gfail("cudaStreamEndCapture", e);
@@ -448,11 +514,85 @@ int sp_group_step(sp_group* g, void* stream) {
         return SP_ERR_CUDA;
     }
     for (auto* b : g->batches) {
-        b->launches += 8;
+        if (g->mt == 0) b->launches += 8;
         b->fresh = false;
+    }
+    if (g->mt > 0) g->launches += 8;
+    return SP_OK;
+}
+
+int sp_group_worklist_bytes(const sp_group* g, int64_t* out) {
+    if (!g || !out) return SP_ERR_ARG;
+    *out = 0;
+    for (int mt : {64, 128}) {  // 64-thread items are the more numerous
+        if (!group_multi_ok(g, mt)) continue;
+        std::vector<sp::fused::MultiClass> c;
+        std::vector<sp::fused::MultiItem> r, k;
+        group_lists(g, mt, c, r, k);
+        const int64_t b = (int64_t)list_bytes(c.size(), r.size(), k.size());
+        if (b > *out) *out = b;
     }
     return SP_OK;
 }
+
+int sp_group_bind(sp_group* g, void* buffer) {
+    if (!g) return SP_ERR_ARG;
+    if (!buffer || ((uintptr_t)buffer % 256)) {
+        g->err = "sp_group_bind: null or not 256-byte aligned buffer";
+        return SP_ERR_ARG;
+    }
+    g->wl = buffer;
+    return SP_OK;
+}
+
+int sp_group_set_worklist(sp_group* g, int mt) {
+    if (!g) return SP_ERR_ARG;
+    if (mt == g->mt) return SP_OK;
+    if (g->exec) {
+        cudaGraphExecDestroy(g->exec);
+        g->exec = nullptr;
+    }
+    if (mt == 0) {
+        g->mt = 0;
+        return SP_OK;
+    }
+    if (!g->wl) {
+        g->err = "sp_group_set_worklist: sp_group_bind first";
+        return SP_ERR_STATE;
+    }
+    for (const sp_batch* b : g->batches)
+        if (!b->bound) {
+            g->err = "sp_group_set_worklist: every batch must be bound";
+            return SP_ERR_STATE;
+        }
+    if (!group_multi_ok(g, mt)) {
+        g->err = "sp_group_set_worklist: classes of one precision, n a power of two with "
+                 "n/16 <= mt and 16 mt/n <= n (mt 64: n = 32..1024, 128: 64..1024)";
+        return SP_ERR_UNSUPPORTED;
+    }
+    std::vector<sp::fused::MultiClass> c;
+    std::vector<sp::fused::MultiItem> r, k;
+    group_lists(g, mt, c, r, k);
+    g->off_rows = al256(c.size() * sizeof(sp::fused::MultiClass));
+    g->off_cols = g->off_rows + al256(r.size() * sizeof(sp::fused::MultiItem));
+    char* base = (char*)g->wl;
+    cudaError_t e;
+    if ((e = sp::fused::multi_prepare(g->batches[0]->fp64, mt)) ||
+        (e = cudaMemcpy(base, c.data(), c.size() * sizeof(c[0]), cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(base + g->off_rows, r.data(), r.size() * sizeof(r[0]), cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(base + g->off_cols, k.data(), k.size() * sizeof(k[0]), cudaMemcpyHostToDevice))) {
+        g->err = std::string("sp_group_set_worklist: ") + cudaGetErrorString(e);
+        return SP_ERR_CUDA;
+    }
+    g->nrow = (int)r.size();
+    g->ncol = (int)k.size();
+    g->mt = mt;
+    return SP_OK;
+}
+
+int sp_group_worklist(const sp_group* g) { return g ? g->mt : -1; }
+
+int64_t sp_group_kernel_launches(const sp_group* g) { return g ? g->launches : -1; }
 
 const char* sp_group_last_error(const sp_group* g) { return g ? g->err.c_str() : "null handle"; }
 

@@ -368,6 +368,106 @@ cudaError_t take_stream_error(unsigned* bits) {
     return cudaSuccess;
 }
 
+// ---- work-list passes
+namespace {
+constexpr int kMaxDevicesMulti = 64;
+struct MultiLaunch {
+    int grid[2][2][2] = {};  // [fp64][mt == 128][column]
+};
+MultiLaunch g_multi[kMaxDevicesMulti];
+
+template <typename T, int MT>
+cudaError_t multi_prepare_t(int dev) {
+    int nsm = 0, occ = 0;
+    cudaError_t e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev))) return e;
+    const int rs = (int)multi_smem<cplx<T>, MT>(), cs = (int)multi_smem<Pair<T>, MT>();
+    if ((e = cudaFuncSetAttribute(k_row_multi<T, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs)))
+        return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_row_multi<T, MT>, MT, rs))) return e;
+    g_multi[dev].grid[sizeof(T) == 8][MT == 128][0] = nsm * (occ > 0 ? occ : 1);
+    auto col = [&](auto kern) -> cudaError_t {
+        cudaError_t e2 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, cs);
+        if (e2) return e2;
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, MT, cs);
+    };
+    if ((e = col(k_col_multi<T, MT, 0>)) || (e = col(k_col_multi<T, MT, 1>)) ||
+        (e = col(k_col_multi<T, MT, 2>)) || (e = col(k_col_multi<T, MT, 3>)))
+        return e;
+    g_multi[dev].grid[sizeof(T) == 8][MT == 128][1] = nsm * (occ > 0 ? occ : 1);
+    return cudaSuccess;
+}
+
+template <typename T, int MT>
+cudaError_t row_multi_t(const void* cls, const void* items, int nitems, int grid, cudaStream_t st) {
+    k_row_multi<T, MT><<<grid, MT, multi_smem<cplx<T>, MT>(), st>>>(
+        (const MultiClass*)cls, (const MultiItem*)items, nitems);
+    return cudaGetLastError();
+}
+
+template <typename T, int MT>
+cudaError_t col_multi_t(int stage, const void* cls, const void* items, int nitems, int grid,
+                        cudaStream_t st) {
+    const size_t sm = multi_smem<Pair<T>, MT>();
+    auto c = (const MultiClass*)cls;
+    auto it = (const MultiItem*)items;
+    switch (stage) {
+        case 0: k_col_multi<T, MT, 0><<<grid, MT, sm, st>>>(c, it, nitems); break;
+        case 1: k_col_multi<T, MT, 1><<<grid, MT, sm, st>>>(c, it, nitems); break;
+        case 2: k_col_multi<T, MT, 2><<<grid, MT, sm, st>>>(c, it, nitems); break;
+        case 3: k_col_multi<T, MT, 3><<<grid, MT, sm, st>>>(c, it, nitems); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+}  // namespace
+
+bool multi_supported(int n, int mt) {
+    if (mt != 64 && mt != 128) return false;
+    if (n < 32 || n > 1024 || (n & (n - 1))) return false;
+    return n / 16 <= mt && 16 * mt / n <= n;
+}
+
+cudaError_t multi_prepare(int fp64, int mt) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e) return e;
+    if (dev >= kMaxDevicesMulti) return cudaErrorInvalidDevice;
+    if (mt == 64) return fp64 ? multi_prepare_t<double, 64>(dev) : multi_prepare_t<float, 64>(dev);
+    if (mt == 128) return fp64 ? multi_prepare_t<double, 128>(dev) : multi_prepare_t<float, 128>(dev);
+    return cudaErrorInvalidValue;
+}
+
+int multi_grid(int fp64, int mt, bool column) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev >= kMaxDevicesMulti) return 0;
+    return g_multi[dev].grid[fp64 ? 1 : 0][mt == 128 ? 1 : 0][column ? 1 : 0];
+}
+
+cudaError_t row_multi(int fp64, int mt, const void* classes, const void* items, int nitems,
+                      cudaStream_t st) {
+    const int grid = multi_grid(fp64, mt, false);
+    if (grid < 1) return cudaErrorNotReady;  // multi_prepare was not called on this device
+    const int g = nitems < grid ? nitems : grid;
+    if (mt == 64) return fp64 ? row_multi_t<double, 64>(classes, items, nitems, g, st)
+                              : row_multi_t<float, 64>(classes, items, nitems, g, st);
+    if (mt == 128) return fp64 ? row_multi_t<double, 128>(classes, items, nitems, g, st)
+                               : row_multi_t<float, 128>(classes, items, nitems, g, st);
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t col_multi(int fp64, int mt, int stage, const void* classes, const void* items,
+                      int nitems, cudaStream_t st) {
+    const int grid = multi_grid(fp64, mt, true);
+    if (grid < 1) return cudaErrorNotReady;
+    const int g = nitems < grid ? nitems : grid;
+    if (mt == 64) return fp64 ? col_multi_t<double, 64>(stage, classes, items, nitems, g, st)
+                              : col_multi_t<float, 64>(stage, classes, items, nitems, g, st);
+    if (mt == 128) return fp64 ? col_multi_t<double, 128>(stage, classes, items, nitems, g, st)
+                               : col_multi_t<float, 128>(stage, classes, items, nitems, g, st);
+    return cudaErrorInvalidValue;
+}
+
 bool supported(int n, int fp64) {
     if (n < 16 || (n & (n - 1))) return false;
     return fp64 ? n <= 4096 : n <= 8192;

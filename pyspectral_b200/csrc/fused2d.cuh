@@ -23,6 +23,7 @@
 
 #include "common.cuh"
 #include "fft_block.cuh"
+#include "fused2d.h"
 #include "reduce.cuh"
 #include "tma.cuh"
 
@@ -135,22 +136,21 @@ struct RowSingle {
     static constexpr size_t smem_bytes(size_t elem) { return (size_t)B * FftPlan<N>::SMEM * elem; }
 };
 
-// Batched launches: blockIdx.y selects the member; each member's arrays start `stride`
-// elements after the previous member's (stride 0 for a single run).
-template <typename T, int N, int BX = 1>
-__global__ void __launch_bounds__(RowSingle<N, BX>::THREADS, 2) k_row_pass(
-    Pair<T>* __restrict__ X, int kc, const cplx<T>* __restrict__ tw, size_t x_stride) {
-    using F = RowSingle<N, BX>;
-    constexpr int TT = F::T;
+// The row pass of B consecutive rows row0 .. row0 + B - 1 of one run's X, by the CTA's
+// B (n/16)-thread sub-blocks (every thread of the CTA calls it: barriers inside); smem_raw
+// holds B exchange buffers.
+template <typename T, int N, int B>
+__device__ __forceinline__ void row_pass_rows(Pair<T>* __restrict__ X, int row0,
+                                              const cplx<T>* __restrict__ tw,
+                                              unsigned char* smem_raw) {
+    constexpr int TT = N / 16;
     constexpr int RI = first_radix<N, true>();   // inverse input pattern
     constexpr int RF = last_radix<N, false>();   // forward output pattern
     static_assert(last_radix<N, true>() == first_radix<N, false>(), "register hand-off");
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int sub = threadIdx.x / TT, t = threadIdx.x % TT;
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
-    const int row = blockIdx.x * F::B + sub;  // n is a multiple of B
+    const int row = row0 + sub;
     const int p = row >> 1, half = row & 1;
-    X += blockIdx.y * x_stride;
 
     static_assert(RI == 16, "first inverse pass is radix 16: slot m holds k = t + m n/16");
     constexpr int KC = (N + 2) / 3;  // == kc: the dealiased columns, fixed by n
@@ -201,6 +201,17 @@ __global__ void __launch_bounds__(RowSingle<N, BX>::THREADS, 2) k_row_pass(
             Xo[2 * k] = o;
         }
     }
+}
+
+// Batched launches: blockIdx.y selects the member; each member's arrays start `stride`
+// elements after the previous member's (stride 0 for a single run).
+template <typename T, int N, int BX = 1>
+__global__ void __launch_bounds__(RowSingle<N, BX>::THREADS, 2) k_row_pass(
+    Pair<T>* __restrict__ X, int kc, const cplx<T>* __restrict__ tw, size_t x_stride) {
+    using F = RowSingle<N, BX>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    (void)kc;  // fixed by n: (n + 2) / 3
+    row_pass_rows<T, N, F::B>(X + blockIdx.y * x_stride, blockIdx.x * F::B, tw, smem_raw);
 }
 
 // CFL bound from the stage-0 inputs: max |u|, max |v| over the physical rows (no write-back).
@@ -322,26 +333,24 @@ __device__ __forceinline__ void col_update(Pair<T> (&v)[16], int t, int ky, bool
 
 // STAGE 0..3: Lawson stage; STAGE = -1: set-up (no forward transform, no update: the inputs of
 // stage 0 from the state u0t).
-template <typename T, int N, int STAGE, int BX = 1>
-__global__ void __launch_bounds__(Fused2D<N, BX>::THREADS) k_col_pass(
-    Pair<T>* __restrict__ X, int kc, cplx<T>* __restrict__ u0t, cplx<T>* __restrict__ acct,
-    const T* __restrict__ tab, const StepParams<T>* __restrict__ P,
-    const cplx<T>* __restrict__ tw, size_t x_stride, size_t u_stride, int tab_stride) {
-    using F = Fused2D<N, BX>;
-    constexpr int TT = F::T;
+// The column pass of columns ky0 .. ky0 + B - 1 of one run (B (n/16)-thread sub-blocks;
+// every thread of the CTA calls it: barriers inside).  Sub-blocks past kc take part in every
+// barrier and write nothing.
+template <typename T, int N, int STAGE, int B>
+__device__ __forceinline__ void col_pass_cols(Pair<T>* __restrict__ X, int kc,
+                                              cplx<T>* __restrict__ u0t,
+                                              cplx<T>* __restrict__ acct,
+                                              const T* __restrict__ tab, const StepParams<T>& p,
+                                              const cplx<T>* __restrict__ tw, int ky0,
+                                              unsigned char* smem_raw) {
+    constexpr int TT = N / 16;
     constexpr int RF0 = first_radix<N, false>();  // forward input pattern
     constexpr int RIL = last_radix<N, true>();    // inverse output pattern
     static_assert(first_radix<N, true>() == last_radix<N, false>(), "register hand-off");
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int sub = threadIdx.x / TT, t = threadIdx.x % TT;
     Pair<T>* sm = reinterpret_cast<Pair<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
-    const int ky = blockIdx.x * F::B + sub;
-    const bool active = ky < kc;  // inactive sub-blocks still take part in every barrier
-    X += blockIdx.y * x_stride;
-    u0t += blockIdx.y * u_stride;
-    acct += blockIdx.y * u_stride;
-    tab += blockIdx.y * tab_stride;
-    const StepParams<T> p = P[blockIdx.y];
+    const int ky = ky0 + sub;
+    const bool active = ky < kc;
 
     Pair<T> v[16];
     if constexpr (STAGE >= 0) {
@@ -366,6 +375,20 @@ __global__ void __launch_bounds__(Fused2D<N, BX>::THREADS) k_col_pass(
                 X[xidx(x, ky, kc)] = v[g * RIL + m];
             }
     }
+}
+
+template <typename T, int N, int STAGE, int BX = 1>
+__global__ void __launch_bounds__(Fused2D<N, BX>::THREADS) k_col_pass(
+    Pair<T>* __restrict__ X, int kc, cplx<T>* __restrict__ u0t, cplx<T>* __restrict__ acct,
+    const T* __restrict__ tab, const StepParams<T>* __restrict__ P,
+    const cplx<T>* __restrict__ tw, size_t x_stride, size_t u_stride, int tab_stride) {
+    using F = Fused2D<N, BX>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const StepParams<T> p = P[blockIdx.y];
+    col_pass_cols<T, N, STAGE, F::B>(X + blockIdx.y * x_stride, kc, u0t + blockIdx.y * u_stride,
+                                     acct + blockIdx.y * u_stride,
+                                     tab + blockIdx.y * tab_stride, p, tw, blockIdx.x * F::B,
+                                     smem_raw);
 }
 
 // ------------------------------------------------------------------------------- streamed column pass
@@ -495,6 +518,86 @@ __global__ void __launch_bounds__(32) k_wait_probe(unsigned* __restrict__ err, u
     const bool ok = tc::mbar_wait(&bar, 0, polls);
     if (!__syncthreads_and(ok) && threadIdx.x == 0) atomicOr(err, kStreamTimeout);
 }
+
+// ------------------------------------------------------------------------------- work lists
+// Persistent passes of a batched group over a packed list of items, one launch per phase for
+// every size class: a CTA of MT threads takes items blockIdx.x, blockIdx.x + gridDim.x, ...;
+// an item is 16 MT / n rows (or columns) of one member, so every item fills the CTA and uses
+// the same shared memory whatever its n.  The row and column work per item is the single-run
+// passes' own (row_pass_rows, col_pass_cols).
+template <int MT, int N>
+constexpr bool multi_fits() {
+    return N >= 16 && (N & (N - 1)) == 0 && N / 16 <= MT && 16 * MT / N <= N;
+}
+
+template <typename T, int MT, int N>
+__device__ __forceinline__ void row_item(const fused::MultiClass& c, const fused::MultiItem& it,
+                                         unsigned char* smem) {
+    if constexpr (multi_fits<MT, N>())
+        row_pass_rows<T, N, 16 * MT / N>(reinterpret_cast<Pair<T>*>(c.X) + (size_t)it.member * c.x_stride,
+                                         it.first, reinterpret_cast<const cplx<T>*>(c.tw), smem);
+}
+
+template <typename T, int MT, int N, int STAGE>
+__device__ __forceinline__ void col_item(const fused::MultiClass& c, const fused::MultiItem& it,
+                                         unsigned char* smem) {
+    if constexpr (multi_fits<MT, N>()) {
+        const size_t m = (size_t)it.member;
+        const StepParams<T> p = reinterpret_cast<const StepParams<T>*>(c.params)[m];
+        col_pass_cols<T, N, STAGE, 16 * MT / N>(
+            reinterpret_cast<Pair<T>*>(c.X) + m * c.x_stride, c.kc,
+            reinterpret_cast<cplx<T>*>(c.u0t) + m * c.u_stride,
+            reinterpret_cast<cplx<T>*>(c.acct) + m * c.u_stride,
+            reinterpret_cast<const T*>(c.tab) + m * (size_t)c.tab_stride, p,
+            reinterpret_cast<const cplx<T>*>(c.tw), it.first, smem);
+    }
+}
+
+template <typename T, int MT>
+__global__ void __launch_bounds__(MT, 1024 / MT) k_row_multi(const fused::MultiClass* __restrict__ cls,
+                                                             const fused::MultiItem* __restrict__ items,
+                                                             int nitems) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+        const fused::MultiItem it = items[w];
+        const fused::MultiClass c = cls[it.cls];
+        switch (c.n) {  // uniform over the CTA: one item is one class
+            case 32: row_item<T, MT, 32>(c, it, smem_raw); break;
+            case 64: row_item<T, MT, 64>(c, it, smem_raw); break;
+            case 128: row_item<T, MT, 128>(c, it, smem_raw); break;
+            case 256: row_item<T, MT, 256>(c, it, smem_raw); break;
+            case 512: row_item<T, MT, 512>(c, it, smem_raw); break;
+            case 1024: row_item<T, MT, 1024>(c, it, smem_raw); break;
+            default: break;
+        }
+        __syncthreads();  // the next item reuses the exchange buffers
+    }
+}
+
+template <typename T, int MT, int STAGE>
+__global__ void __launch_bounds__(MT, 512 / MT) k_col_multi(const fused::MultiClass* __restrict__ cls,
+                                                            const fused::MultiItem* __restrict__ items,
+                                                            int nitems) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+        const fused::MultiItem it = items[w];
+        const fused::MultiClass c = cls[it.cls];
+        switch (c.n) {
+            case 32: col_item<T, MT, 32, STAGE>(c, it, smem_raw); break;
+            case 64: col_item<T, MT, 64, STAGE>(c, it, smem_raw); break;
+            case 128: col_item<T, MT, 128, STAGE>(c, it, smem_raw); break;
+            case 256: col_item<T, MT, 256, STAGE>(c, it, smem_raw); break;
+            case 512: col_item<T, MT, 512, STAGE>(c, it, smem_raw); break;
+            case 1024: col_item<T, MT, 1024, STAGE>(c, it, smem_raw); break;
+            default: break;
+        }
+        __syncthreads();
+    }
+}
+
+// Shared memory of one work-list CTA: 16 MT / n exchange buffers of n + n/16 elements.
+template <typename E, int MT>
+constexpr size_t multi_smem() { return (size_t)MT * 17 * sizeof(E); }
 
 // ------------------------------------------------------------------------------- layout moves
 // u0 (n, nh) NumPy layout -> u0t (kc, n): 32 x 32 tiles through shared memory.

@@ -45,6 +45,37 @@ cudaError_t col_pass(int n, int fp64, int stage, void* X, int kc, void* u0t, voi
                      const void* tab, const void* params, const void* tw, cudaStream_t st,
                      int members = 1, size_t x_stride = 0, size_t u_stride = 0,
                      int tab_stride = 0, int tile = 1);
+// ---- work-list passes of a batched group: one launch per phase over every size class.
+// One size class as the work-list passes see it: member 0's arrays; member m's start m times
+// the stride later (X in Pair units, u0t / acct in complex units, tab in reals).
+struct MultiClass {
+    void* X;
+    void* u0t;
+    void* acct;
+    const void* tab;
+    const void* params;  // one StepParams per member
+    const void* tw;
+    uint64_t x_stride, u_stride;
+    int tab_stride, n, kc, pad;
+};
+// One item: rows (row pass) or columns (column pass) first .. first + 16 mt / n - 1 of member
+// `member` of class `cls`, for a CTA of mt threads.
+struct MultiItem {
+    int cls, member, first;
+};
+// Sizes the work-list passes run for CTAs of mt (64 or 128) threads: a power of two with
+// n / 16 <= mt and 16 mt / n <= n (an item holds whole rows of one member).
+bool multi_supported(int n, int mt);
+inline int multi_per_item(int n, int mt) { return 16 * mt / n; }
+// Dynamic shared memory opt-in and the persistent grids (SMs x resident CTAs) of the passes;
+// once per process, outside any stream capture.
+cudaError_t multi_prepare(int fp64, int mt);
+int multi_grid(int fp64, int mt, bool column);
+cudaError_t row_multi(int fp64, int mt, const void* classes, const void* items, int nitems,
+                      cudaStream_t st);
+cudaError_t col_multi(int fp64, int mt, int stage, const void* classes, const void* items,
+                      int nitems, cudaStream_t st);
+
 cudaError_t transpose_in(int fp64, const void* u0, void* u0t, int n, int kc, cudaStream_t st,
                          int members = 1, size_t u0_stride = 0, size_t u_stride = 0);
 cudaError_t transpose_out(int fp64, const void* u0t, void* u0, int n, int kc, cudaStream_t st,

@@ -120,6 +120,46 @@ class TileTuner:
         return best
 
 
+    def choose_worklist(self, ens: Ensemble) -> int:
+        """The group step's form: the work-list passes with CTAs of 64 or 128 threads, or one
+        launch per class and phase (0) — whichever steps the group fastest (CUDA events,
+        ``reps`` group steps after two warm-up steps); cached per GPU model and class set."""
+        torch, lib = ens.torch, ens.lib
+        gpu = torch.cuda.get_device_name(ens.device)
+        sig = ",".join(f"{c.n}{'d' if c.fp64 else 'f'}x{c.count}" for c in ens.classes)
+        key = f"{gpu}|group|{sig}"
+        cands = [0] + [mt for mt in (64, 128) if ens._worklist_ok(mt)]
+        hit = self.cache.get(key)
+        if isinstance(hit, dict) and hit.get("worklist") in cands:
+            self.report[key] = dict(hit, cached=True)
+            return int(hit["worklist"])
+        if len(cands) == 1:
+            return 0
+        st = ens._stream()
+        for c in ens.classes:
+            c.set_step(np.full(c.count, 1e-4), np.zeros(c.count), st)
+            c._check(lib.sp_batch_prepare(c.h, st), "sp_batch_prepare")
+        cur = torch.cuda.current_stream(ens.device)
+        times: dict[int, float] = {}
+        for mt in cands:
+            ens.set_worklist(mt)
+            for _ in range(2):
+                ens._gcheck(lib.sp_group_step(ens._group, st), "sp_group_step")
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(cur)
+            for _ in range(self.reps):
+                ens._gcheck(lib.sp_group_step(ens._group, st), "sp_group_step")
+            e1.record(cur)
+            e1.synchronize()
+            times[mt] = e0.elapsed_time(e1) / self.reps
+        best = min(times, key=times.get)
+        entry = {"worklist": best, "ms_per_step": {str(k): v for k, v in times.items()}}
+        self.cache[key] = entry
+        self.report[key] = dict(entry, cached=False)
+        save_tune_cache(self.path, self.cache)
+        return best
+
+
 class _SizeClass:
     """One batched engine: the members of one (n, dtype) class."""
 
@@ -186,10 +226,15 @@ class Ensemble:
     ``members``: one :class:`Config` per run (dim 2; n a power of two, 16..8192 fp32 /
     16..4096 fp64).  Runs of the same n and dtype form a size class and must share drag and
     forcing band; viscosity, time step and forcing amplitude are per run.  ``autotune``: pick
-    each class's tile with :class:`TileTuner` (default on, see PYSPECTRAL_B200_AUTOTUNE).
+    each class's tile and the group's work-list CTA size with :class:`TileTuner` (default on,
+    see PYSPECTRAL_B200_AUTOTUNE).  ``worklist``: the group step as one persistent launch per
+    phase over a packed work list of every class (``sp_group_set_worklist``: 64 or 128 threads
+    per CTA; 0 = one launch per class and phase; None = the tuner's choice, else 64), where the
+    classes allow it (one precision, n = 32..1024).
     """
 
-    def __init__(self, members: Sequence[Config], autotune: bool | None = None) -> None:
+    def __init__(self, members: Sequence[Config], autotune: bool | None = None,
+                 worklist: int | None = None) -> None:
         import torch
 
         from pyspectral_b200.solver import _cuda_reason
@@ -232,6 +277,21 @@ class Ensemble:
             raise _lib.EngineError("sp_group_create failed")
         self._group = g
         self._gfin = weakref.finalize(self, lib.sp_group_destroy, ctypes.c_void_p(g))
+        # the work list: a caller-owned device buffer, CTA size tuned or given
+        nbytes = ctypes.c_int64(0)
+        self._gcheck(lib.sp_group_worklist_bytes(g, ctypes.byref(nbytes)), "sp_group_worklist_bytes")
+        self._wl = None
+        if nbytes.value > 0:
+            self._wl = torch.zeros(int(nbytes.value), dtype=torch.uint8, device=self.device)
+            self._gcheck(lib.sp_group_bind(g, _lib.dptr(self._wl)), "sp_group_bind")
+            if worklist is None:
+                worklist = self.tuner.choose_worklist(self) if self.tuner is not None else 64
+            if worklist and not self._worklist_ok(int(worklist)):
+                worklist = 0
+            self.set_worklist(int(worklist or 0))
+        elif worklist:
+            raise BackendUnavailable("ensemble: these size classes have no work-list path "
+                                     "(one precision, n = 32..1024)")
         self.t = np.zeros(len(self.members))
         self.nstep = 0
         self.force_amp = np.array([c.force_amp for c in self.members], dtype=np.float64)
@@ -240,6 +300,26 @@ class Ensemble:
     # ------------------------------------------------------------------ plumbing
     def __len__(self) -> int:
         return len(self.members)
+
+    def _gcheck(self, status: int, what: str) -> None:
+        if status != 0:
+            msg = (self.lib.sp_group_last_error(self._group) or b"").decode()
+            raise _lib.EngineError(f"{what} failed ({_lib.STATUS_NAMES.get(status)}): {msg}")
+
+    def _worklist_ok(self, mt: int) -> bool:
+        fp = {c.fp64 for c in self.classes}
+        return len(fp) == 1 and all(32 <= c.n <= 1024 and c.n // 16 <= mt and 16 * mt // c.n <= c.n
+                                    for c in self.classes)
+
+    def set_worklist(self, mt: int) -> None:
+        """Step the group through the work-list passes with CTAs of mt threads (64 or 128), or
+        through one launch per class and phase (mt = 0)."""
+        self._gcheck(self.lib.sp_group_set_worklist(self._group, int(mt)), "sp_group_set_worklist")
+
+    @property
+    def worklist(self) -> int:
+        """CTA threads of the work-list passes in use; 0 when each class launches its own."""
+        return int(self.lib.sp_group_worklist(self._group))
 
     def _stream(self) -> ctypes.c_void_p:
         return ctypes.c_void_p(self.torch.cuda.current_stream(self.device).cuda_stream)
@@ -366,4 +446,5 @@ class Ensemble:
 
     @property
     def kernel_launches(self) -> int:
-        return int(sum(self.lib.sp_batch_kernel_launches(c.h) for c in self.classes))
+        return int(sum(self.lib.sp_batch_kernel_launches(c.h) for c in self.classes)
+                   + self.lib.sp_group_kernel_launches(self._group))

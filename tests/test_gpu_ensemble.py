@@ -115,15 +115,62 @@ def test_constant_power_cfl_run_matches_single_run_driver():
         assert np.abs(ens.get_state(i) - r).max() / np.abs(r).max() < 1e-12
 
 
-def test_one_graph_step_launches_eight_kernels_per_class():
+@pytest.mark.parametrize("worklist", [0, 64])
+def test_one_graph_step_launch_count(worklist):
+    """Per class: 8 launches per class and step; work list: 8 for the whole group (a row pass
+    and a column pass per RK stage over every class)."""
     from pyspectral_b200.ensemble import Ensemble
 
-    ens = Ensemble(_members("float32"))
+    ens = Ensemble(_members("float32"), autotune=False, worklist=worklist)
+    assert ens.worklist == worklist
     ens.set_states(_ics(ens.members))
     ens.step(1e-3)
     before = ens.kernel_launches
     ens.step(1e-3)
-    assert ens.kernel_launches - before == 8 * len(ens.classes) == 24
+    assert ens.kernel_launches - before == (8 if worklist else 8 * len(ens.classes))
+
+
+def _uneven(dtype):
+    return [Config(n=n, dim=2, nu=1e-3 * (1 + 0.3 * j), alpha=0.1, alpha_kmax=2.0,
+                   force_amp=0.2 + 0.05 * j, force_klo=3, force_khi=5, dtype=dtype)
+            for n in (64, 128, 256, 512, 1024) for j in range(3 if n < 1024 else 1)]
+
+
+@pytest.mark.parametrize("dtype,mt", [("float32", 64), ("float32", 128), ("float64", 64),
+                                      ("float64", 128)])
+def test_worklist_group_step_equals_per_class_launches(dtype, mt):
+    """The packed work list runs each row and column with the single-run passes' code:
+    members equal the per-class launches over dt and amplitude changes, to round-off (the
+    kernels are compiled separately and may contract multiply-adds differently)."""
+    from pyspectral_b200.ensemble import Ensemble
+
+    cfgs = _uneven(dtype)
+    ics = _ics(cfgs)
+    a = Ensemble(cfgs, autotune=False, worklist=0)
+    b = Ensemble(cfgs, autotune=False, worklist=mt)
+    assert b.worklist == mt
+    for e in (a, b):
+        e.set_states(ics)
+    for k in range(4):
+        dt = np.array([2e-4 * (1 + 0.1 * i + 0.05 * k) for i in range(len(cfgs))])
+        amps = np.array([0.2 + 0.01 * i + 0.02 * k for i in range(len(cfgs))])
+        for e in (a, b):
+            e.set_forcing_amplitudes(amps)
+            e.step(dt)
+    tol = 1e-13 if dtype == "float64" else 1e-6
+    for i in range(len(cfgs)):
+        ra = a.get_state(i)
+        assert np.abs(b.get_state(i) - ra).max() <= tol * np.abs(ra).max(), i
+
+
+def test_worklist_rejects_classes_it_does_not_run():
+    from pyspectral_b200.ensemble import Ensemble
+
+    cfgs = [Config(n=2048, dim=2, nu=1e-4, dtype="float32"), Config(n=64, dim=2, nu=1e-3)]
+    e = Ensemble(cfgs, autotune=False)
+    assert e.worklist == 0  # 2048^2 and a second precision: one launch per class
+    with pytest.raises(BackendUnavailable):
+        Ensemble(cfgs, autotune=False, worklist=64)
 
 
 def test_ensemble_rejects_unsupported_members():

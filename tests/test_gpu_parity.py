@@ -69,15 +69,17 @@ def test_matches_oracle(v, dtype, dim, form, alpha_kmax):
     assert err < TOL[dtype], err
 
 
+@pytest.mark.parametrize("variant", ["b200", "b200/fused-fft-graph"])
 @pytest.mark.parametrize("dim,form", [(2, "basdevant"), (3, "basdevant"), (3, "rotational")])
 @pytest.mark.parametrize("akm", [0.0, 2.0])
-def test_matches_reference_vectors(dim, form, akm):
-    """Against the arrays the reference's NumpySolver produced (tests/golden)."""
+def test_matches_reference_vectors(dim, form, akm, variant):
+    """Against the arrays the reference's NumpySolver produced (tests/golden), on the cuFFT
+    engine and on the hand-written fused FFT engine."""
     n = 32 if dim == 2 else 16
     key = f"parity_{dim}d_{form}_akm{int(akm)}"
     cfg = Config(n=n, dim=dim, nu=0.01, alpha=0.5, alpha_kmax=akm, force_amp=0.3, force_klo=1,
                  force_khi=2.5, dtype="float64", form=form)
-    s = get("b200").make(cfg)
+    s = get(variant).make(cfg)
     s.set_state(GOLDEN[key + "_ic"])
     s.advance(5, 0.01)
     s.set_forcing_amplitude(0.1)
