@@ -13,8 +13,11 @@
 // Elements are either one complex sequence (cplx<T>) or two sequences sharing the transform
 // (Pair<T>).  Twiddles come from a per-pass table (FftPlan::tw_offset, built in fp64 on the
 // host and rounded to T); the forward transform conjugates them.  DIR = +1: inverse (e^{+}),
-// DIR = -1: forward.
+// DIR = -1: forward.  For N = 2 16^k, split_inverse / split_forward (below) run the transform
+// as two length-N/2 halves joined by a radix-2 step whose partners trade through warp shuffles.
 #pragma once
+
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -384,12 +387,15 @@ __device__ __forceinline__ void pass_compute_h(E (&v)[16], int t, const C* __res
 
 // Full transform.  On entry v holds the input in the pattern of pass 0 (in_pos with radix
 // radix(INV, 0)); on exit v holds the output at in_pos with the last pass's radix.  `sm` is this
-// sequence's padded shared buffer; every thread of the CTA must call (barriers inside).
-template <int N, bool INV, bool WARP = false, typename E, typename C>
+// sequence's padded shared buffer; every thread of the CTA must call (barriers inside).  TWINV
+// picks the table blocks: a forward transform whose passes have the inverse's radices and
+// strides (N = 16^k) may read the inverse blocks, conjugated.
+template <int N, bool INV, bool WARP = false, bool TWINV = INV, typename E, typename C>
 __device__ __forceinline__ void block_fft(E (&v)[16], E* sm, int t, const C* __restrict__ tw) {
     using P = FftPlan<N>;
     static_assert(!WARP || P::T <= 32, "a warp-synchronised transform fits in one warp");
     constexpr int DIR = INV ? 1 : -1;
+    static_assert(TWINV == INV || P::R0 == 1, "shared blocks need equal pass structures");
     constexpr int R0 = P::radix(INV, 0), S0 = P::stride(INV, 0);
     pass_compute<N, R0, S0, DIR>(v, t, tw);  // S0 = 1: no twiddles
     if constexpr (P::NP > 1) {
@@ -398,21 +404,21 @@ __device__ __forceinline__ void block_fft(E (&v)[16], E* sm, int t, const C* __r
         seq_sync<WARP>();
         pass_load<N, R1>(v, sm, t);
         seq_sync<WARP>();
-        pass_compute_h<N, R1, S1, DIR>(v, t, tw + P::tw_offset(INV, 1));
+        pass_compute_h<N, R1, S1, DIR>(v, t, tw + P::tw_offset(TWINV, 1));
         if constexpr (P::NP > 2) {
             constexpr int R2 = P::radix(INV, 2), S2 = P::stride(INV, 2);
             pass_store<N, R1, S1>(v, sm, t);
             seq_sync<WARP>();
             pass_load<N, R2>(v, sm, t);
             seq_sync<WARP>();
-            pass_compute_h<N, R2, S2, DIR>(v, t, tw + P::tw_offset(INV, 2));
+            pass_compute_h<N, R2, S2, DIR>(v, t, tw + P::tw_offset(TWINV, 2));
             if constexpr (P::NP > 3) {
                 constexpr int R3 = P::radix(INV, 3), S3 = P::stride(INV, 3);
                 pass_store<N, R2, S2>(v, sm, t);
                 seq_sync<WARP>();
                 pass_load<N, R3>(v, sm, t);
                 seq_sync<WARP>();
-                pass_compute_h<N, R3, S3, DIR>(v, t, tw + P::tw_offset(INV, 3));
+                pass_compute_h<N, R3, S3, DIR>(v, t, tw + P::tw_offset(TWINV, 3));
             }
         }
     }
@@ -441,28 +447,168 @@ __device__ __forceinline__ void exchange_halves(Pair<T> (&v)[16], cplx<T>* sm, i
 
 // block_fft of Pair elements with the exchanges of exchange_halves: `sm` holds
 // FftPlan<N>::SMEM complex values instead of Pairs.
-template <int N, bool INV, bool WARP = false, typename T, typename C>
+template <int N, bool INV, bool WARP = false, bool TWINV = INV, typename T, typename C>
 __device__ __forceinline__ void block_fft_halves(Pair<T> (&v)[16], cplx<T>* sm, int t,
                                                  const C* __restrict__ tw) {
     using P = FftPlan<N>;
+    static_assert(TWINV == INV || P::R0 == 1, "shared blocks need equal pass structures");
     constexpr int DIR = INV ? 1 : -1;
     constexpr int R0 = P::radix(INV, 0), S0 = P::stride(INV, 0);
     pass_compute<N, R0, S0, DIR>(v, t, tw);
     if constexpr (P::NP > 1) {
         constexpr int R1 = P::radix(INV, 1), S1 = P::stride(INV, 1);
         exchange_halves<N, R0, S0, R1, WARP>(v, sm, t);
-        pass_compute_h<N, R1, S1, DIR>(v, t, tw + P::tw_offset(INV, 1));
+        pass_compute_h<N, R1, S1, DIR>(v, t, tw + P::tw_offset(TWINV, 1));
         if constexpr (P::NP > 2) {
             constexpr int R2 = P::radix(INV, 2), S2 = P::stride(INV, 2);
             exchange_halves<N, R1, S1, R2, WARP>(v, sm, t);
-            pass_compute_h<N, R2, S2, DIR>(v, t, tw + P::tw_offset(INV, 2));
+            pass_compute_h<N, R2, S2, DIR>(v, t, tw + P::tw_offset(TWINV, 2));
             if constexpr (P::NP > 3) {
                 constexpr int R3 = P::radix(INV, 3), S3 = P::stride(INV, 3);
                 exchange_halves<N, R2, S2, R3, WARP>(v, sm, t);
-                pass_compute_h<N, R3, S3, DIR>(v, t, tw + P::tw_offset(INV, 3));
+                pass_compute_h<N, R3, S3, DIR>(v, t, tw + P::tw_offset(TWINV, 3));
             }
         }
     }
+}
+
+// ---------------------------------------------------------------------------- split transforms
+// A transform of length N = 2 M, M = 16^k (N = 32, 512, 8192), as two length-M halves, one per
+// half of the sequence's T = N/16 threads, joined by one radix-2 step:
+//   inverse (decimation in time): the halves transform the even and the odd inputs (E, O) and
+//     x_n = E_n + w^n O_n, x_{n+M} = E_n - w^n O_n, w = exp(2 pi i / N);
+//   forward (decimation in frequency): a_j = x_j + x_{j+M}, b_j = (x_j - x_{j+M}) w^-j, and
+//     the halves transform a (the even outputs) and b (the odd outputs).
+// A thread's role r: half h = r / (T/2), sub-role s = r mod (T/2).  The radix-2 step needs E_n and
+// O_n in one thread while the halves leave them in roles s and s + T/2, so each thread keeps
+// eight of its sixteen values and trades the other eight with role r ^ (T/2).  split_role puts
+// the two roles in lanes l and l ^ 16 of one warp (T > 32: bits 4 and log2(T) - 1 of the
+// thread index swapped; T <= 32: lanes l and l ^ (T/2)): eight warp shuffles of one element
+// instead of a shared-memory exchange of sixteen, on each side of the pointwise work.
+// Patterns: the inverse takes element tau + m N/16 in slot m and the forward leaves element
+// tau + m N/16 in slot m, tau = split_tau(r) = 2 s + h; in between, slot 2g holds x_j and slot
+// 2g + 1 holds x_{j+M}, j = r + T g.  Table: FftPlan<N>'s; the halves' passes (radix 16,
+// strides 1, 16, 256) are its first inverse passes, and its radix-2 block holds w^js, js < M.
+template <int N>
+constexpr bool split_plan() { return FftPlan<N>::R0 == 2; }
+
+template <int T>
+__device__ __forceinline__ int split_role(int p) {
+    if constexpr (T <= 32) {
+        return p;
+    } else {
+        constexpr int HB = ilog2(T) - 1;
+        const int b4 = (p >> 4) & 1, bt = (p >> HB) & 1;
+        return (p & ~((1 << 4) | (1 << HB))) | (b4 << HB) | (bt << 4);
+    }
+}
+
+template <int T>
+__device__ __forceinline__ int split_tau(int r) { return 2 * (r % (T / 2)) + r / (T / 2); }
+
+template <typename T>
+__device__ __forceinline__ T shfl_xor_e(T x, int lm) { return __shfl_xor_sync(0xffffffffu, x, lm); }
+__device__ __forceinline__ float2 shfl_xor_e(float2 x, int lm) {
+    return make_float2(shfl_xor_e(x.x, lm), shfl_xor_e(x.y, lm));
+}
+__device__ __forceinline__ double2 shfl_xor_e(double2 x, int lm) {
+    return make_double2(shfl_xor_e(x.x, lm), shfl_xor_e(x.y, lm));
+}
+template <typename T>
+__device__ __forceinline__ Pair<T> shfl_xor_e(Pair<T> x, int lm) {
+    return {shfl_xor_e(x.a, lm), shfl_xor_e(x.b, lm)};
+}
+
+// Half h = 0 keeps the even slots and takes its partner's even slots into its odd ones; half
+// h = 1 keeps the odd slots and takes its partner's odd slots into its even ones.
+template <int T, typename E>
+__device__ __forceinline__ void half_trade(E (&v)[16], int h) {
+    constexpr int LM = T > 32 ? 16 : T / 2;
+#pragma unroll
+    for (int g = 0; g < 8; ++g) {
+        const E got = shfl_xor_e(h ? v[2 * g] : v[2 * g + 1], LM);
+        if (h) v[2 * g] = got;
+        else v[2 * g + 1] = got;
+    }
+}
+
+template <int G, typename E, typename C>
+__device__ __forceinline__ void dif_radix2_group(E (&v)[16], const C w1) {
+    if constexpr (G < 8) {
+        dft2<-1>(v + G * 2);
+        v[G * 2 + 1] = emul(v[G * 2 + 1], rot16<-1, G>(w1));
+        dif_radix2_group<G + 1>(v, w1);
+    }
+}
+
+template <int N>
+constexpr bool split_tables_agree() {
+    using P = FftPlan<N>;
+    using Q = FftPlan<N / 2>;
+    for (int p = 1; p < Q::NP; ++p)
+        if (Q::tw_offset(true, p) != P::tw_offset(true, p)) return false;
+    return P::radix(true, P::NP - 1) == 2 && P::stride(true, P::NP - 1) == N / 2;
+}
+
+// One half's transform of a split transform: block_fft when the buffer holds the element type,
+// block_fft_halves for Pair elements exchanged through a buffer of single complex values.
+template <int N, bool INV, bool WARP, bool TWINV, typename E, typename S, typename C>
+__device__ __forceinline__ void half_fft(E (&v)[16], S* sm, int s, const C* __restrict__ tw) {
+    if constexpr (std::is_same_v<E, S>) block_fft<N, INV, WARP, TWINV>(v, sm, s, tw);
+    else block_fft_halves<N, INV, WARP, TWINV>(v, sm, s, tw);
+}
+
+// Inverse split transform: slot m holds element split_tau(r) + m N/16 on entry; slot 2g holds
+// x_j and slot 2g + 1 holds x_{j + N/2}, j = r + (N/16) g, on exit.  `sm`: FftPlan<N>::SMEM
+// elements or, for Pair elements, single complex values (the two halves' buffers); every
+// thread of the CTA calls (barriers inside).
+template <int N, bool WARP = false, typename E, typename S, typename C>
+__device__ __forceinline__ void split_inverse(E (&v)[16], S* sm, int r, const C* __restrict__ tw) {
+    static_assert(split_plan<N>() && split_tables_agree<N>(), "N = 2 16^k");
+    using P = FftPlan<N>;
+    constexpr int H = P::T / 2;
+    const int h = r / H;
+    half_fft<N / 2, true, WARP, true>(v, sm + h * FftPlan<N / 2>::SMEM, r - h * H, tw);
+    half_trade<P::T>(v, h);
+    radix2_half_group<1, 0>(v, tw_load<1>(tw + P::tw_offset(true, P::NP - 1), r));
+}
+
+// Forward split transform: the exit pattern of split_inverse on entry; slot m holds element
+// split_tau(r) + m N/16 on exit.
+template <int N, bool WARP = false, typename E, typename S, typename C>
+__device__ __forceinline__ void split_forward(E (&v)[16], S* sm, int r, const C* __restrict__ tw) {
+    static_assert(split_plan<N>() && split_tables_agree<N>(), "N = 2 16^k");
+    using P = FftPlan<N>;
+    constexpr int H = P::T / 2;
+    const int h = r / H;
+    dif_radix2_group<0>(v, tw_load<-1>(tw + P::tw_offset(true, P::NP - 1), r));
+    half_trade<P::T>(v, h);
+    half_fft<N / 2, false, WARP, true>(v, sm + h * FftPlan<N / 2>::SMEM, r - h * H, tw);
+}
+
+// The transform of one sequence by thread t of its N/16: the split form when N = 2 16^k,
+// block_fft (or block_fft_halves for Pair elements through a single complex buffer) otherwise.
+// Frequency side (inverse input, forward output): slot m holds index spec_base(t) + m N/16.
+// Sample side (inverse output, forward input): slot g R + m holds in_pos<N, R>(phys_base(t),
+// g, m), R = last_radix<N, true>() = first_radix<N, false>().
+template <int N, bool INV, bool WARP = false, typename E, typename S, typename C>
+__device__ __forceinline__ void seq_fft(E (&v)[16], S* sm, int t, const C* __restrict__ tw) {
+    if constexpr (split_plan<N>()) {
+        if constexpr (INV) split_inverse<N, WARP>(v, sm, split_role<N / 16>(t), tw);
+        else split_forward<N, WARP>(v, sm, split_role<N / 16>(t), tw);
+    } else {
+        half_fft<N, INV, WARP, INV>(v, sm, t, tw);
+    }
+}
+template <int N>
+__device__ __forceinline__ int spec_base(int t) {
+    if constexpr (split_plan<N>()) return split_tau<N / 16>(split_role<N / 16>(t));
+    else return t;
+}
+template <int N>
+__device__ __forceinline__ int phys_base(int t) {
+    if constexpr (split_plan<N>()) return split_role<N / 16>(t);
+    else return t;
 }
 
 // radix of the last pass (output pattern) and of the first pass (input pattern)

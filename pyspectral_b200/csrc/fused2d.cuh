@@ -154,21 +154,29 @@ __device__ __forceinline__ void row_pass_rows(Pair<T>* __restrict__ X, int row0,
 
     static_assert(RI == 16, "first inverse pass is radix 16: slot m holds k = t + m n/16");
     constexpr int KC = (N + 2) / 3;  // == kc: the dealiased columns, fixed by n
+    // n = 2 16^k: split transforms (fft_block.cuh), whose slot m holds k = k0 + m n/16 on input
+    // and output with k0 = spec_base(t); otherwise k0 = t.
+    constexpr bool SPLIT = split_plan<N>();
+    const int k0 = spec_base<N>(t);
     cplx<T> v[16];
-    row_inputs<T, N>(v, X + (size_t)p * KC * 2 + half, t);
-    block_fft<N, true>(v, sm, t, tw);
+    row_inputs<T, N>(v, X + (size_t)p * KC * 2 + half, k0);
+    seq_fft<N, true>(v, sm, t, tw);
     // physical space: z = u + i v  ->  (v^2 - u^2) + i (u v)
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
         T u = v[e].x, w = v[e].y;
         v[e] = mk<T>((w - u) * (w + u), u * w);
     }
-    __syncthreads();
-    block_fft<N, false>(v, sm, t, tw);
-    __syncthreads();
+    if constexpr (SPLIT) {
+        seq_fft<N, false>(v, sm, t, tw);  // its last shared reads end at a barrier
+    } else {
+        __syncthreads();
+        seq_fft<N, false>(v, sm, t, tw);
+        __syncthreads();
+    }
     static_assert(RF == 16, "last forward pass is radix 16: slot m holds k = t + m n/16");
     {
-        cplx<T>* st = sm + spad(t);
+        cplx<T>* st = sm + spad(k0);
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             const int c = m * TT;
@@ -293,20 +301,22 @@ __device__ __forceinline__ Pair<T> next_inputs(T kx, T ky, T k2, bool keep, cplx
 }
 
 // The pointwise middle of a column pass, on the forward transform's output held in registers:
-// v[g*RL + m] belongs to row index i = in_pos<N, RL>(t, g, m).  Nonlinear term, Lawson stage
-// update of u0t / acct, and the next inverse-transform inputs written back into v.
+// v[m] belongs to row index i = k0 + m n/16 (the forward's last pass is radix 16; k0 =
+// spec_base(t)).  Nonlinear term, Lawson stage update of u0t / acct, and the next
+// inverse-transform inputs written back into v.
 template <typename T, int N, int STAGE>
-__device__ __forceinline__ void col_update(Pair<T> (&v)[16], int t, int ky, bool active,
+__device__ __forceinline__ void col_update(Pair<T> (&v)[16], int k0, int ky, bool active,
                                            cplx<T>* __restrict__ u0t, cplx<T>* __restrict__ acct,
                                            const T* __restrict__ tab, const StepParams<T>& p) {
     constexpr int RL = last_radix<N, false>();
+    static_assert(RL == 16, "slot m holds row index k0 + m n/16");
     const T kyr = (T)ky;
     const int nh = N / 2 + 1;
 #pragma unroll
     for (int g = 0; g < 16 / RL; ++g)
 #pragma unroll
         for (int m = 0; m < RL; ++m) {
-            const int i = in_pos<N, RL>(t, g, m);
+            const int i = in_pos<N, RL>(k0, g, m);
             const int kxi = signed_k(i, N);
             const int akx = kxi < 0 ? -kxi : kxi;
             const bool keep = active && (3 * akx < N);
@@ -351,6 +361,8 @@ __device__ __forceinline__ void col_pass_cols(Pair<T>* __restrict__ X, int kc,
     Pair<T>* sm = reinterpret_cast<Pair<T>*>(smem_raw) + sub * FftPlan<N>::SMEM;
     const int ky = ky0 + sub;
     const bool active = ky < kc;
+    // rows x = in_pos(xb, g, m) at the ends, k0 + m n/16 in the middle (see seq_fft)
+    const int xb = phys_base<N>(t), k0 = spec_base<N>(t);
 
     Pair<T> v[16];
     if constexpr (STAGE >= 0) {
@@ -358,20 +370,20 @@ __device__ __forceinline__ void col_pass_cols(Pair<T>* __restrict__ X, int kc,
         for (int g = 0; g < 16 / RF0; ++g)
 #pragma unroll
             for (int m = 0; m < RF0; ++m) {
-                const int x = in_pos<N, RF0>(t, g, m);
+                const int x = in_pos<N, RF0>(xb, g, m);
                 v[g * RF0 + m] = active ? X[xidx(x, ky, kc)] : Pair<T>{mk<T>(0, 0), mk<T>(0, 0)};
             }
-        block_fft<N, false>(v, sm, t, tw);
+        seq_fft<N, false>(v, sm, t, tw);
     }
-    col_update<T, N, STAGE>(v, t, ky, active, u0t, acct, tab, p);
+    col_update<T, N, STAGE>(v, k0, ky, active, u0t, acct, tab, p);
     __syncthreads();
-    block_fft<N, true>(v, sm, t, tw);
+    seq_fft<N, true>(v, sm, t, tw);
     if (active) {
 #pragma unroll
         for (int g = 0; g < 16 / RIL; ++g)
 #pragma unroll
             for (int m = 0; m < RIL; ++m) {
-                const int x = in_pos<N, RIL>(t, g, m);
+                const int x = in_pos<N, RIL>(xb, g, m);
                 X[xidx(x, ky, kc)] = v[g * RIL + m];
             }
     }
@@ -444,6 +456,7 @@ k_col_stream(const __grid_constant__ CUtensorMap xmap, Pair<T>* __restrict__ X, 
     cplx<T>* ex = reinterpret_cast<cplx<T>*>(stream_smem + CS::PB_BYTES);
     uint64_t* bar = reinterpret_cast<uint64_t*>(stream_smem + CS::PB_BYTES + CS::EX_BYTES);
     const int t = threadIdx.x;
+    const int xb = phys_base<N>(t), k0 = spec_base<N>(t);  // see seq_fft
     const StepParams<T> p = *P;
 
     // kept rows of a state column: i < LO and i >= HI (|kx| < n/3), rounded out to 16 bytes
@@ -487,20 +500,20 @@ k_col_stream(const __grid_constant__ CUtensorMap xmap, Pair<T>* __restrict__ X, 
 #pragma unroll
         for (int g = 0; g < 16 / RF0; ++g)
 #pragma unroll
-            for (int m = 0; m < RF0; ++m) v[g * RF0 + m] = pb[in_pos<N, RF0>(t, g, m)];
+            for (int m = 0; m < RF0; ++m) v[g * RF0 + m] = pb[in_pos<N, RF0>(xb, g, m)];
         __syncthreads();  // every thread has its column: the buffer may be refilled
         if (t == 0 && ky + (int)gridDim.x < kc) {
             tc::fence_smem_to_async();
             fetch(ky + gridDim.x);
         }
-        block_fft_halves<N, false>(v, ex, t, tw);
-        col_update<T, N, STAGE>(v, t, ky, true, u0t, acct, tab, p);
-        block_fft_halves<N, true>(v, ex, t, tw);
+        seq_fft<N, false>(v, ex, t, tw);
+        col_update<T, N, STAGE>(v, k0, ky, true, u0t, acct, tab, p);
+        seq_fft<N, true>(v, ex, t, tw);
 #pragma unroll
         for (int g = 0; g < 16 / RIL; ++g)
 #pragma unroll
             for (int m = 0; m < RIL; ++m)
-                st_stream(X + xidx(in_pos<N, RIL>(t, g, m), ky, (N + 2) / 3), v[g * RIL + m]);
+                st_stream(X + xidx(in_pos<N, RIL>(xb, g, m), ky, (N + 2) / 3), v[g * RIL + m]);
     }
 }
 

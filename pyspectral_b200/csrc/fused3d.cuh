@@ -80,8 +80,8 @@ __device__ __forceinline__ void for_slots(F&& f) {
     for_slots_impl(f, std::make_integer_sequence<int, 16>{});
 }
 
-// Register slot M of the first inverse pass / last forward pass (radix 16) holds FFT index
-// k = t + M n/16.  Kind of the slot against the kept set [0, KM] u [n - KM, n): 0 = all kept
+// Register slot M on the frequency side of a transform (inverse input, forward output) holds
+// FFT index k = k0 + M n/16, k0 = spec_base(thread) < n/16.  Kind of the slot against the kept set [0, KM] u [n - KM, n): 0 = all kept
 // low, 1 = all kept high, 2 = none kept, 3 = mixed (decided per thread).
 template <int N, int M>
 constexpr int slot_kind() {
@@ -94,9 +94,9 @@ constexpr int slot_kind() {
 
 // value of slot M: load_lo(k) for a kept low k, load_hi(k) for a kept high k, else zero
 template <int N, int M, typename E, typename Lo, typename Hi>
-__device__ __forceinline__ E slot_value(int t, Lo&& load_lo, Hi&& load_hi, E zero) {
+__device__ __forceinline__ E slot_value(int k0, Lo&& load_lo, Hi&& load_hi, E zero) {
     constexpr int kind = slot_kind<N, M>();
-    const int k = t + M * (N / 16);
+    const int k = k0 + M * (N / 16);
     if constexpr (kind == 0) return load_lo(k);
     else if constexpr (kind == 1) return load_hi(k);
     else if constexpr (kind == 2) return zero;
@@ -109,9 +109,9 @@ __device__ __forceinline__ E slot_value(int t, Lo&& load_lo, Hi&& load_hi, E zer
 
 // store(k) for slot M when its k is kept
 template <int N, int M, typename St>
-__device__ __forceinline__ void slot_store(int t, St&& store) {
+__device__ __forceinline__ void slot_store(int k0, St&& store) {
     constexpr int kind = slot_kind<N, M>();
-    const int k = t + M * (N / 16);
+    const int k = k0 + M * (N / 16);
     if constexpr (kind == 0 || kind == 1) store(k);
     else if constexpr (kind == 3) {
         if (k <= Dims<N>::KM || k >= N - Dims<N>::KM) store(k);
@@ -172,20 +172,21 @@ __global__ void __launch_bounds__(y_threads<T>()) k3_yinv(const Pair<T>* __restr
     const bool active = unit < units;
     const YUnit yu = y_unit<N>(unit, nfields);
     const int x = yu.x, f = yu.f, q = yu.q;
+    const int kb = spec_base<N>(t), yb = phys_base<N>(t);
     Pair<T> v[16];
     for_slots([&](auto mc) {
         constexpr int M = decltype(mc)::value;
         auto lo = [&](int k) { return Bs[spec_idx<N, ROT>(x, f, k, q)]; };
         auto hi = [&](int k) { return Bs[spec_idx<N, ROT>(x, f, k - N + D::KK, q)]; };
-        v[M] = active ? slot_value<N, M>(t, lo, hi, pzero<T>()) : pzero<T>();
+        v[M] = active ? slot_value<N, M>(kb, lo, hi, pzero<T>()) : pzero<T>();
     });
-    block_fft_halves<N, true, true>(v, exch[seq], t, tw);
+    seq_fft<N, true, true>(v, exch[seq], t, tw);
     if (active) {
 #pragma unroll
         for (int g = 0; g < 16 / RIL; ++g)
 #pragma unroll
             for (int m = 0; m < RIL; ++m)
-                Bp[phys_idx<N, ROT>(x, f, in_pos<N, RIL>(t, g, m), q)] = v[g * RIL + m];
+                Bp[phys_idx<N, ROT>(x, f, in_pos<N, RIL>(yb, g, m), q)] = v[g * RIL + m];
     }
 }
 
@@ -204,18 +205,19 @@ __global__ void __launch_bounds__(y_threads<T>()) k3_yfwd(const Pair<T>* __restr
     const bool active = unit < units;
     const YUnit yu = y_unit<N>(unit, nfields);
     const int x = yu.x, f = yu.f, q = yu.q;
+    const int kb = spec_base<N>(t), yb = phys_base<N>(t);
     Pair<T> v[16];
 #pragma unroll
     for (int g = 0; g < 16 / RF0; ++g)
 #pragma unroll
         for (int m = 0; m < RF0; ++m)
             v[g * RF0 + m] =
-                active ? Bp[phys_idx<N, ROT>(x, f, in_pos<N, RF0>(t, g, m), q)] : pzero<T>();
-    block_fft_halves<N, false, true>(v, exch[seq], t, tw);
+                active ? Bp[phys_idx<N, ROT>(x, f, in_pos<N, RF0>(yb, g, m), q)] : pzero<T>();
+    seq_fft<N, false, true>(v, exch[seq], t, tw);
     if (active) {
         for_slots([&](auto mc) {
             constexpr int M = decltype(mc)::value;
-            slot_store<N, M>(t, [&](int k) { Bs[spec_idx<N, ROT>(x, f, kept_of_fft<N>(k), q)] = v[M]; });
+            slot_store<N, M>(kb, [&](int k) { Bs[spec_idx<N, ROT>(x, f, kept_of_fft<N>(k), q)] = v[M]; });
         });
     }
 }
@@ -264,6 +266,7 @@ __global__ void __launch_bounds__(z_threads<T>()) k3_z(Pair<T>* __restrict__ Bp,
     };
     cplx<T>* sm = exch[seq];
     const cplx<T> z0 = mk<T>(0, 0);
+    const int kb = spec_base<N>(t);  // the z line's samples stay in registers: no sample index
 
     Pair<T> v[16];
     if constexpr (ROT && MODE == 0) {
@@ -273,9 +276,9 @@ __global__ void __launch_bounds__(z_threads<T>()) k3_z(Pair<T>* __restrict__ Bp,
             constexpr int M = decltype(mc)::value;
             auto lo = [&](int k) { return herm_pair_lo<T>(B[at(4, k)], B[at(5, k)], k); };
             auto hi = [&](int k) { return herm_pair_hi<T>(B[at(4, N - k)], B[at(5, N - k)]); };
-            w[M] = active ? slot_value<N, M>(t, lo, hi, z0) : z0;
+            w[M] = active ? slot_value<N, M>(kb, lo, hi, z0) : z0;
         });
-        block_fft<N, true, true>(w, sm, t, tw);
+        seq_fft<N, true, true>(w, sm, t, tw);
 #pragma unroll
         for (int e = 0; e < 16; ++e) stash[e][threadIdx.x] = w[e];
     }
@@ -298,9 +301,9 @@ __global__ void __launch_bounds__(z_threads<T>()) k3_z(Pair<T>* __restrict__ Bp,
             }
             return Pair<T>{herm_pair_hi<T>(B[at(0, kk)], B[at(1, kk)]), wz};
         };
-        v[M] = active ? slot_value<N, M>(t, lo, hi, pzero<T>()) : pzero<T>();
+        v[M] = active ? slot_value<N, M>(kb, lo, hi, pzero<T>()) : pzero<T>();
     });
-    block_fft_halves<N, true, true>(v, sm, t, tw);  // v[e] = (u + i v, w + i (omega_x or 0))
+    seq_fft<N, true, true>(v, sm, t, tw);  // v[e] = (u + i v, w + i (omega_x or 0))
 
     if (want_max) {
         double mu = 0.0, mv = 0.0, mw = 0.0;
@@ -348,7 +351,7 @@ __global__ void __launch_bounds__(z_threads<T>()) k3_z(Pair<T>* __restrict__ Bp,
                 v[e].b = mk<T>(u * vv, u * w);
             }
         }
-        block_fft_halves<N, false, true>(v, sm, t, tw);  // output slot M: k = t + M n/16
+        seq_fft<N, false, true>(v, sm, t, tw);  // output slot M: k = kb + M n/16
         // split Z' = F(p + i q): P(k) = (Z'(k) + conj Z'(n-k)) / 2,
         // Q(k) = (Z'(k) - conj Z'(n-k)) / 2i
         constexpr int NSPLIT = ROT ? 1 : 2;
@@ -356,7 +359,7 @@ __global__ void __launch_bounds__(z_threads<T>()) k3_z(Pair<T>* __restrict__ Bp,
         for (int h = 0; h < NSPLIT; ++h) {
             __syncwarp();
 #pragma unroll
-            for (int e = 0; e < 16; ++e) sm[spad(t + e * TT)] = h == 0 ? v[e].a : v[e].b;
+            for (int e = 0; e < 16; ++e) sm[spad(kb + e * TT)] = h == 0 ? v[e].a : v[e].b;
             __syncwarp();
 #pragma unroll
             for (int j = 0; j < (D::KZ + TT - 1) / TT; ++j) {
@@ -373,7 +376,7 @@ __global__ void __launch_bounds__(z_threads<T>()) k3_z(Pair<T>* __restrict__ Bp,
             if (active) {
                 for_slots([&](auto mc) {
                     constexpr int M = decltype(mc)::value;
-                    const int k = t + M * TT;
+                    const int k = kb + M * TT;
                     if (M * TT < D::KZ && k < D::KZ) B[at(2, k)] = v[M].b;
                 });
             }
@@ -382,11 +385,11 @@ __global__ void __launch_bounds__(z_threads<T>()) k3_z(Pair<T>* __restrict__ Bp,
             cplx<T> w[16];
 #pragma unroll
             for (int e = 0; e < 16; ++e) w[e] = stash[e][threadIdx.x];  // (v w, 0)
-            block_fft<N, false, true>(w, sm, t, tw);
+            seq_fft<N, false, true>(w, sm, t, tw);
             if (active) {
                 for_slots([&](auto mc) {
                     constexpr int M = decltype(mc)::value;
-                    const int k = t + M * TT;
+                    const int k = kb + M * TT;
                     if (M * TT < D::KZ && k < D::KZ) B[at(4, k)] = w[M];
                 });
             }
@@ -444,6 +447,7 @@ __global__ void __launch_bounds__(XPass<T, N, ROT>::THREADS, 2) k3_x(
     const long unit = (long)blockIdx.x * U + sub;
     const bool active = unit < X::UNITS;
     const int q = (int)(unit % D::NQ), kyi = (int)(unit / D::NQ);
+    const int kb = spec_base<N>(t), xb = phys_base<N>(t);
     const StepParams<T> p = *P;
     auto st_at = [&](int s, int f, int kxi) -> Pair<T>& {
         return stage[((size_t)s * NF + f) * KK + kxi];
@@ -458,12 +462,12 @@ __global__ void __launch_bounds__(XPass<T, N, ROT>::THREADS, 2) k3_x(
             for (int g = 0; g < 16 / RF0; ++g)
 #pragma unroll
                 for (int m = 0; m < RF0; ++m)
-                    v[g * RF0 + m] = active ? Bs[spec_idx<N, ROT>(in_pos<N, RF0>(t, g, m), f, kyi, q)]
+                    v[g * RF0 + m] = active ? Bs[spec_idx<N, ROT>(in_pos<N, RF0>(xb, g, m), f, kyi, q)]
                                             : pzero<T>();
-            block_fft_halves<N, false, true>(v, sm, t, tw);
+            seq_fft<N, false, true>(v, sm, t, tw);
             for_slots([&](auto mc) {
                 constexpr int M = decltype(mc)::value;
-                slot_store<N, M>(t, [&](int k) { st_at(sub, f, kept_of_fft<N>(k)) = v[M]; });
+                slot_store<N, M>(kb, [&](int k) { st_at(sub, f, kept_of_fft<N>(k)) = v[M]; });
             });
         }
         __syncthreads();
@@ -562,15 +566,15 @@ __global__ void __launch_bounds__(XPass<T, N, ROT>::THREADS, 2) k3_x(
             constexpr int M = decltype(mc)::value;
             auto lo = [&](int k) { return st_at(sub, f, k); };
             auto hi = [&](int k) { return st_at(sub, f, k - N + KK); };
-            v[M] = slot_value<N, M>(t, lo, hi, pzero<T>());
+            v[M] = slot_value<N, M>(kb, lo, hi, pzero<T>());
         });
-        block_fft_halves<N, true, true>(v, sm, t, tw);
+        seq_fft<N, true, true>(v, sm, t, tw);
         if (active) {
 #pragma unroll
             for (int g = 0; g < 16 / RIL; ++g)
 #pragma unroll
                 for (int m = 0; m < RIL; ++m)
-                    Bs[spec_idx<N, ROT>(in_pos<N, RIL>(t, g, m), f, kyi, q)] = v[g * RIL + m];
+                    Bs[spec_idx<N, ROT>(in_pos<N, RIL>(xb, g, m), f, kyi, q)] = v[g * RIL + m];
         }
     }
 }
