@@ -756,6 +756,55 @@ def ours_ensemble(args, w: dict) -> int:
     return 0
 
 
+def ensemble_secondary(wname: str, steps: int, warmup: int, local: int) -> dict:
+    """The uneven-ensemble workload measured inside the default bench run on one GPU: the
+    autotuned Ensemble stepped with per-member CFL dt and constant-power forcing, CUDA-event
+    ms/step over ``steps`` steps after ``warmup``, its own clock samples, the aggregate FFT
+    roofline (batched cuFFT of every class + pointwise bytes at the copy bandwidth) and the
+    tuner's choices."""
+    import torch
+
+    from pyspectral_b200.ensemble import Ensemble
+
+    w = WORKLOADS[wname]
+    members = ensemble_members(w)
+    ens = Ensemble(members)
+    ens.set_states(ensemble_ics(w, members))
+    ens.run_steps(warmup, cfl=w["cfl"], target_power=w["power"])
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = ens.kernel_launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    ens.run_steps(steps, cfl=w["cfl"], target_power=w["power"])
+    ev1.record()
+    ev1.synchronize()
+    clk = clocks.stop()
+    ms_step = ev0.elapsed_time(ev1) / steps
+    launches = ens.kernel_launches - l0
+    pts = sum(float(c.n) ** 2 for c in members)
+    engine = ("work list" if ens.worklist else "per-class launches, one group graph")
+    tiles = {str(c.n): c.tile for c in ens.classes}
+    report = None if ens.tuner is None else {k: dict(v) for k, v in ens.tuner.report.items()}
+    del ens
+    gc.collect()
+    torch.cuda.empty_cache()
+    t_fft_stage = ensemble_fft_stage_ms(w)
+    bcopy = copy_bandwidth_gbs()
+    pw = sum(w["per_size"] * traffic_model(n, 2, "basdevant", w["dtype"])["pointwise_bytes"]
+             for n in w["sizes"])
+    t_roof = 4 * t_fft_stage + pw / (bcopy * 1e9) * 1e3
+    return {
+        "workload": wname, "sizes": list(w["sizes"]), "runs_per_size": w["per_size"],
+        "dtype": "f32" if w["dtype"] == "float32" else "f64", "steps": steps, "warmup": warmup,
+        "ms_per_step": ms_step, "value": pts / (ms_step * 1e-3) / 1e6, "unit": "Mpts/s",
+        "pct_fft_roofline": 100.0 * t_roof / ms_step, "t_roofline_step_ms": t_roof,
+        "engine": engine, "tiles": tiles, "autotune": report, "gpu_launches": launches,
+        "clocks": clk,
+    }
+
+
 def ours_closure(args, w: dict) -> int:
     """The learned-closure workload: the whole study (batched 2048^2 DNS data, training,
     validation, a-posteriori test on held-out seeds) on one GPU; the headline is the wall-time
@@ -1068,6 +1117,8 @@ def ours(args, w: dict) -> int:
     if world == 1 and args.workload == "decay2d-8192-fp32" and not args.no_secondary:
         # the 3D Taylor-Green step at 512^3 beside the 2D headline, timed in the same run
         line["secondary"] = secondary_line("tgv3d-512-fp32-basdevant", 10, 3, local)
+        # and the 256-member uneven ensemble (64 runs each of 128^2 .. 1024^2)
+        line["secondary_ensemble"] = ensemble_secondary("ensemble-4x64-fp32", 20, 3, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = time_oracle(w, 1, 1)
         line["cpu_baseline"] = {
