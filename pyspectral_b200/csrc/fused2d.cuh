@@ -181,7 +181,7 @@ __device__ __forceinline__ void row_pass_rows(Pair<T>* __restrict__ X, int row0,
         for (int m = 0; m < 16; ++m) {
             const int c = m * TT;
             if (c % 16 == 0) st[c + (c >> 4)] = v[m];
-            else sm[spad(t + c)] = v[m];
+            else sm[spad(k0 + c)] = v[m];
         }
     }
     __syncthreads();
