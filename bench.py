@@ -699,9 +699,16 @@ def ours_ensemble(args, w: dict) -> int:
     comm.barrier()
     t0 = time.perf_counter()
     e2.set_states(ics)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
     e2.run_steps(args.steps, cfl=w["cfl"], target_power=w["power"])
-    outs = [e2.ens.get_state(i) for i in range(len(e2.local))] if e2.ens is not None else []
-    e2e_s = comm.max(time.perf_counter() - t0)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    outs = e2.ens.get_states() if e2.ens is not None else []
+    t3 = time.perf_counter()
+    e2e_s = comm.max(t3 - t0)
+    e2e_parts = {"set_states_s": comm.max(t1 - t0), "steps_s": comm.max(t2 - t1),
+                 "get_states_s": comm.max(t3 - t2)}
     state_bytes = sum(c.u0.nbytes for c in e2.ens.classes) if e2.ens is not None else 0
     state_bytes = int(comm.max(float(state_bytes)) * world)
     del e2, outs
@@ -739,7 +746,8 @@ def ours_ensemble(args, w: dict) -> int:
         "e2e": {"value": pts * args.steps / e2e_s / 1e6, "unit": "Mpts/s",
                 "h2d_bytes_per_step": state_bytes / args.steps,
                 "d2h_bytes_per_step": state_bytes / args.steps,
-                "what": "set_states(host) + K steps + get_state of every member, wall clock"},
+                "what": "set_states(host) + K steps + get_states (every member), wall clock",
+                "parts": e2e_parts},
         "gpu_launches": launches, "clocks": clk,
         "autotune": None if ens is None or ens.tuner is None else {
             k: dict(v) for k, v in ens.tuner.report.items()},

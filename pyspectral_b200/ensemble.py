@@ -292,6 +292,10 @@ class Ensemble:
         elif worklist:
             raise BackendUnavailable("ensemble: these size classes have no work-list path "
                                      "(one precision, n = 32..1024)")
+        # pinned host staging of set_states / get_states, one buffer per class, and the event
+        # after the last copy from it to the device
+        self._pinned: dict[int, Any] = {}
+        self._staged: dict[int, Any] = {}
         self.t = np.zeros(len(self.members))
         self.nstep = 0
         self.force_amp = np.array([c.force_amp for c in self.members], dtype=np.float64)
@@ -338,12 +342,19 @@ class Ensemble:
         if len(states) != len(self.members):
             raise ValueError("one state per member")
         for i, a in enumerate(states):
-            ci, slot = self.where[i]
-            c = self.classes[ci]
-            a = np.asarray(a)
-            if a.shape != spectral_shape(c.n, 2):
-                raise ValueError(f"member {i}: state shape {a.shape} != {spectral_shape(c.n, 2)}")
-            c.u0[slot].copy_(self.torch.from_numpy(np.ascontiguousarray(a)).to(c.cdt))
+            c = self.classes[self.where[i][0]]
+            if np.shape(a) != spectral_shape(c.n, 2):
+                raise ValueError(f"member {i}: state shape {np.shape(a)} != "
+                                 f"{spectral_shape(c.n, 2)}")
+        # per class: cast into the pinned staging buffer (torch's threaded copy), one copy to
+        # the device
+        torch = self.torch
+        for ci, c in enumerate(self.classes):
+            stage = self._staging(ci)
+            for slot, i in enumerate(self.index[ci]):
+                stage[slot].copy_(torch.from_numpy(np.ascontiguousarray(states[i])))
+            c.u0.copy_(stage, non_blocking=True)
+            self._staged[ci].record(torch.cuda.current_stream(self.device))
         self._upload(np.where(np.isnan(self.dt), 0.0, self.dt))
         for c in self.classes:
             c._check(self.lib.sp_batch_prepare(c.h, self._stream()), "sp_batch_prepare")
@@ -358,6 +369,50 @@ class Ensemble:
 
     def get_state(self, i: int) -> np.ndarray:
         return self.state_native(i).detach().cpu().numpy().astype(np.complex128)
+
+    def _staging(self, ci: int) -> Any:
+        """Class ci's pinned host buffer (its state's shape and dtype; allocated on first use,
+        reused), once the last copy from it to the device has finished."""
+        torch = self.torch
+        if ci not in self._pinned:
+            c = self.classes[ci]
+            self._pinned[ci] = torch.empty(c.u0.shape, dtype=c.u0.dtype, pin_memory=True)
+            self._staged[ci] = torch.cuda.Event()
+            self._staged[ci].record(torch.cuda.current_stream(self.device))
+        self._staged[ci].synchronize()
+        return self._pinned[ci]
+
+    def get_states(self) -> list[np.ndarray]:
+        """Every member's state (host arrays, NumPy r2c layout, complex128): one state refresh
+        and one device-to-host copy per size class, where get_state refreshes the member's
+        whole class on every call."""
+        from pyspectral_b200.solver import B200Solver
+
+        torch = self.torch
+        stream = torch.cuda.current_stream(self.device)
+        out: list[Any] = [None] * len(self.members)
+        for ci, c in enumerate(self.classes):
+            c._check(self.lib.sp_batch_sync_state(c.h, self._stream()), "sp_batch_sync_state")
+            # through a pinned buffer in chunks: the widening cast of a chunk (torch's threaded
+            # copy) overlaps the PCIe copy of the next
+            stage = self._staging(ci)
+            src, sflat = c.u0.detach().reshape(-1), stage.view(-1)
+            chunks = B200Solver._chunks(sflat.numel())
+            landed = []
+            for lo, hi in chunks:
+                sflat[lo:hi].copy_(src[lo:hi], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+                landed.append(ev)
+            res = torch.empty(c.u0.shape, dtype=torch.complex128)
+            rflat = res.view(-1)
+            for (lo, hi), ev in zip(chunks, landed):
+                ev.synchronize()
+                rflat[lo:hi].copy_(sflat[lo:hi])
+            host = res.numpy()
+            for slot, i in enumerate(self.index[ci]):
+                out[i] = host[slot]
+        return out
 
     # ------------------------------------------------------------------ stepping
     def set_forcing_amplitudes(self, amps: Any) -> None:

@@ -51,6 +51,23 @@ def test_members_equal_single_runs_bit_for_bit(dtype):
         assert ens.t[i] == pytest.approx(s.t)
 
 
+def test_get_states_equals_get_state_of_each_member():
+    """get_states (one refresh and one copy per size class) returns every member's state, in
+    member order, equal bit for bit to get_state of that member."""
+    from pyspectral_b200.ensemble import Ensemble
+
+    cfgs = _members("float32")
+    ens = Ensemble(cfgs, autotune=False)
+    ens.set_states(_ics(cfgs))
+    for k in range(3):
+        ens.step(np.array([1e-3 * (1 + 0.1 * i + 0.05 * k) for i in range(len(cfgs))]))
+    allst = ens.get_states()
+    assert len(allst) == len(cfgs)
+    for i in range(len(cfgs)):
+        assert allst[i].dtype == np.complex128
+        assert np.array_equal(allst[i], ens.get_state(i)), i
+
+
 def test_batched_diagnostics_and_cfl_match_single_runs():
     from pyspectral_b200.ensemble import Ensemble
 
