@@ -304,10 +304,14 @@ __device__ __forceinline__ Pair<T> next_inputs(T kx, T ky, T k2, bool keep, cplx
 // v[m] belongs to row index i = k0 + m n/16 (the forward's last pass is radix 16; k0 =
 // spec_base(t)).  Nonlinear term, Lawson stage update of u0t / acct, and the next
 // inverse-transform inputs written back into v.
-template <typename T, int N, int STAGE>
-__device__ __forceinline__ void col_update(Pair<T> (&v)[16], int k0, int ky, bool active,
-                                           cplx<T>* __restrict__ u0t, cplx<T>* __restrict__ acct,
-                                           const T* __restrict__ tab, const StepParams<T>& p) {
+// ld_u(i, o) / ld_c(i, o): the state / accumulator value of kept row i (o = its global index);
+// the updated values go to global memory.
+template <typename T, int N, int STAGE, typename LdU, typename LdC>
+__device__ __forceinline__ void col_update_from(Pair<T> (&v)[16], int k0, int ky, bool active,
+                                                cplx<T>* __restrict__ u0t,
+                                                cplx<T>* __restrict__ acct,
+                                                const T* __restrict__ tab,
+                                                const StepParams<T>& p, LdU&& ld_u, LdC&& ld_c) {
     constexpr int RL = last_radix<N, false>();
     static_assert(RL == 16, "slot m holds row index k0 + m n/16");
     const T kyr = (T)ky;
@@ -324,14 +328,14 @@ __device__ __forceinline__ void col_update(Pair<T> (&v)[16], int k0, int ky, boo
             cplx<T> nxt = mk<T>(0, 0);
             if (keep) {
                 const size_t o = (size_t)ky * N + i;
-                cplx<T> U = __ldcs(u0t + o);  // streamed once: keep L1 for the twiddles
+                cplx<T> U = ld_u(i, o);
                 if constexpr (STAGE < 0) {
                     nxt = U;
                 } else {
                     Pair<T> e = v[g * RL + m];
                     cplx<T> Nl = axpy(kx * kyr, e.a, scl(kx * kx - kyr * kyr, e.b));
                     IFac<T> f = if_factors(tab, nh, akx, ky, -1, k2, p);
-                    cplx<T> C = STAGE > 0 ? __ldcs(acct + o) : mk<T>(0, 0);
+                    cplx<T> C = STAGE > 0 ? ld_c(i, o) : mk<T>(0, 0);
                     nxt = lawson_stage<T, (STAGE < 0 ? 0 : STAGE)>(p.dt, f, Nl, U, C);
                     if (STAGE == 3) __stcs(u0t + o, nxt);
                     else __stcs(acct + o, C);
@@ -339,6 +343,17 @@ __device__ __forceinline__ void col_update(Pair<T> (&v)[16], int k0, int ky, boo
             }
             v[g * RL + m] = next_inputs<T>(kx, kyr, k2, keep, nxt, p.scale);
         }
+}
+
+// col_update_from with the state and accumulator read from global memory (streamed once:
+// L1 keeps the twiddles).
+template <typename T, int N, int STAGE>
+__device__ __forceinline__ void col_update(Pair<T> (&v)[16], int k0, int ky, bool active,
+                                           cplx<T>* __restrict__ u0t, cplx<T>* __restrict__ acct,
+                                           const T* __restrict__ tab, const StepParams<T>& p) {
+    col_update_from<T, N, STAGE>(v, k0, ky, active, u0t, acct, tab, p,
+                                 [&](int, size_t o) { return __ldcs(u0t + o); },
+                                 [&](int, size_t o) { return __ldcs(acct + o); });
 }
 
 // STAGE 0..3: Lawson stage; STAGE = -1: set-up (no forward transform, no update: the inputs of
@@ -405,10 +420,11 @@ __global__ void __launch_bounds__(Fused2D<N, BX>::THREADS) k_col_pass(
 
 // ------------------------------------------------------------------------------- streamed column pass
 // Persistent form of k_col_pass for one run (stages 0..3): CTA b takes columns b, b + grid, ...
-// While a column is transformed in registers, the next column's X data (n Pairs at a stride of
-// one row pair) is already on its way into shared memory by TMA (boxes of 2 Pairs x up to 256
-// row pairs), and the next column's state / accumulator rows are prefetched into L2, so the
-// column's loads no longer wait on HBM.  The two transforms exchange through a buffer of single
+// The X data of a column (n Pairs at a stride of one row pair) comes into shared memory by TMA
+// (boxes of 2 Pairs x up to 256 row pairs) while the previous column's inverse transform runs;
+// once it is in registers, the same buffer takes the column's kept state / accumulator rows
+// (bulk copies, prefetched into L2 beforehand) while the forward transform runs, so the update
+// reads them from shared memory, and the next column's X data is asked for after the update.  The two transforms exchange through a buffer of single
 // complex values (exchange_halves), which leaves room for the prefetch buffer.  (Exchanging
 // whole Pairs through the prefetch buffer in the forward transform and starting the next copy
 // after it saves half the barriers but leaves the copy too little time: slower at n = 8192.)
@@ -454,6 +470,7 @@ k_col_stream(const __grid_constant__ CUtensorMap xmap, Pair<T>* __restrict__ X, 
     extern __shared__ __align__(128) unsigned char stream_smem[];
     Pair<T>* pb = reinterpret_cast<Pair<T>*>(stream_smem);
     cplx<T>* ex = reinterpret_cast<cplx<T>*>(stream_smem + CS::PB_BYTES);
+    // bar[0]: the X data of a column; bar[1]: its kept state (and accumulator) rows
     uint64_t* bar = reinterpret_cast<uint64_t*>(stream_smem + CS::PB_BYTES + CS::EX_BYTES);
     const int t = threadIdx.x;
     const int xb = phys_base<N>(t), k0 = spec_base<N>(t);  // see seq_fft
@@ -463,8 +480,16 @@ k_col_stream(const __grid_constant__ CUtensorMap xmap, Pair<T>* __restrict__ X, 
     constexpr int EPB = 16 / (int)sizeof(cplx<T>);  // elements per 16 bytes
     constexpr int LO = (((N - 1) / 3 + 1) + EPB - 1) / EPB * EPB;
     constexpr int HI = (N - (N - 1) / 3) / EPB * EPB;
-    // thread 0: ask for column c's X data (completing on `bar`) and its kept state rows in L2
-    auto fetch = [&](int c) {
+    // staged in the X buffer once the column's X data is in registers: [0, LO) then [HI, n)
+    // of the state, the same of the accumulator after them
+    constexpr int KEPT = LO + (N - HI);
+    constexpr uint32_t ROWS_BYTES = (uint32_t)(KEPT * sizeof(cplx<T>));
+    static_assert(2 * (size_t)ROWS_BYTES <= CS::PB_BYTES, "state rows fit the X buffer");
+    cplx<T>* sU = reinterpret_cast<cplx<T>*>(stream_smem);
+    cplx<T>* sC = sU + KEPT;
+    // thread 0: column c's X data into the buffer (completing on bar[0]) and its kept state
+    // rows into L2 (for the copy into shared memory that follows)
+    auto fetch_x = [&](int c) {
         tma::arrive_expect_tx(bar, (uint32_t)CS::PB_BYTES);
 #pragma unroll 1
         for (int b = 0; b < NBOX; ++b)
@@ -476,38 +501,68 @@ k_col_stream(const __grid_constant__ CUtensorMap xmap, Pair<T>* __restrict__ X, 
             tma::prefetch_l2(acct + (size_t)c * N + HI, (uint32_t)((N - HI) * sizeof(cplx<T>)));
         }
     };
+    // thread 0: column c's kept state (and accumulator) rows into the buffer (bar[1])
+    auto fetch_rows = [&](int c) {
+        tma::arrive_expect_tx(bar + 1, (STAGE > 0 ? 2u : 1u) * ROWS_BYTES);
+        tma::load_1d(sU, u0t + (size_t)c * N, (uint32_t)(LO * sizeof(cplx<T>)), bar + 1);
+        tma::load_1d(sU + LO, u0t + (size_t)c * N + HI, (uint32_t)((N - HI) * sizeof(cplx<T>)),
+                     bar + 1);
+        if (STAGE > 0) {
+            tma::load_1d(sC, acct + (size_t)c * N, (uint32_t)(LO * sizeof(cplx<T>)), bar + 1);
+            tma::load_1d(sC + LO, acct + (size_t)c * N + HI,
+                         (uint32_t)((N - HI) * sizeof(cplx<T>)), bar + 1);
+        }
+    };
+    auto srow = [](int i) { return i < LO ? i : LO + (i - HI); };  // kept row -> staged index
 
     int ky = blockIdx.x;
     if (t == 0) {
         tc::mbar_init(bar, 1);
+        tc::mbar_init(bar + 1, 1);
         tma::fence_barrier_init();
     }
     __syncthreads();
-    if (t == 0 && ky < kc) fetch(ky);
-    uint32_t phase = 0;
+    if (t == 0 && ky < kc) fetch_x(ky);
+    uint32_t px = 0, pr = 0;
     for (; ky < kc; ky += gridDim.x) {
-        const bool ok = tc::mbar_wait(bar, phase, kStreamWait);
+        const bool ok = tc::mbar_wait(bar, px, kStreamWait);
         if (!__syncthreads_and(ok)) {
             // the copy never completed: report, give it one more bounded wait, leave
             if (t == 0) {
                 atomicOr(err, kStreamTimeout);
-                tc::mbar_wait(bar, phase, kStreamWait);
+                tc::mbar_wait(bar, px, kStreamWait);
             }
             return;
         }
-        phase ^= 1u;
+        px ^= 1u;
         Pair<T> v[16];
 #pragma unroll
         for (int g = 0; g < 16 / RF0; ++g)
 #pragma unroll
             for (int m = 0; m < RF0; ++m) v[g * RF0 + m] = pb[in_pos<N, RF0>(xb, g, m)];
-        __syncthreads();  // every thread has its column: the buffer may be refilled
-        if (t == 0 && ky + (int)gridDim.x < kc) {
+        __syncthreads();  // every thread has its column: the buffer takes the state rows
+        if (t == 0) {
             tc::fence_smem_to_async();
-            fetch(ky + gridDim.x);
+            fetch_rows(ky);
         }
         seq_fft<N, false>(v, ex, t, tw);
-        col_update<T, N, STAGE>(v, k0, ky, true, u0t, acct, tab, p);
+        const bool ok_rows = tc::mbar_wait(bar + 1, pr, kStreamWait);
+        if (!__syncthreads_and(ok_rows)) {
+            if (t == 0) {
+                atomicOr(err, kStreamTimeout);
+                tc::mbar_wait(bar + 1, pr, kStreamWait);
+            }
+            return;  // the next column's X data was not asked for yet
+        }
+        pr ^= 1u;
+        col_update_from<T, N, STAGE>(v, k0, ky, true, u0t, acct, tab, p,
+                                     [&](int i, size_t) { return sU[srow(i)]; },
+                                     [&](int i, size_t) { return sC[srow(i)]; });
+        __syncthreads();  // every thread has its rows: the buffer may take the next column
+        if (t == 0 && ky + (int)gridDim.x < kc) {
+            tc::fence_smem_to_async();
+            fetch_x(ky + gridDim.x);
+        }
         seq_fft<N, true>(v, ex, t, tw);
 #pragma unroll
         for (int g = 0; g < 16 / RIL; ++g)

@@ -34,6 +34,16 @@ __device__ __forceinline__ void load_2d(void* dst, const void* map, int x, int y
         : "memory");
 }
 
+// `bytes` (a multiple of 16) of global memory at `src` -> shared memory at `dst` (both 16-byte
+// aligned), completing on `bar`.
+__device__ __forceinline__ void load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(tc::smem_u32(dst)), "l"((uint64_t)(uintptr_t)src), "r"(bytes),
+        "r"(tc::smem_u32(bar))
+        : "memory");
+}
+
 // Start moving `bytes` (a multiple of 16, 16-byte aligned source) of global memory into L2.
 __device__ __forceinline__ void prefetch_l2(const void* src, uint32_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((uint64_t)(uintptr_t)src),
