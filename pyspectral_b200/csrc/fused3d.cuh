@@ -38,6 +38,7 @@
 
 #include "common.cuh"
 #include "fft_block.cuh"
+#include "tma.cuh"
 
 namespace sp {
 namespace f3 {
@@ -449,6 +450,26 @@ __global__ void __launch_bounds__(XPass<T, N, ROT>::THREADS, 2) k3_x(
     const int q = (int)(unit % D::NQ), kyi = (int)(unit / D::NQ);
     const int kb = spec_base<N>(t), xb = phys_base<N>(t);
     const StepParams<T> p = *P;
+    // thread 0: the CTA's compact state (and accumulator) rows into L2 while the forward
+    // transforms run (bulk prefetches of whole 16-byte blocks inside each row range)
+    if (threadIdx.x == 0) {
+        constexpr size_t CS = (size_t)KK * D::KZ * KK;  // one component
+        for (int s = 0; s < U; ++s) {
+            const long us = (long)blockIdx.x * U + s;
+            if (us >= X::UNITS) break;
+            const int qs = (int)(us % D::NQ), kyis = (int)(us / D::NQ);
+            const int nkz = D::KZ - 2 * qs < 2 ? D::KZ - 2 * qs : 2;
+            if (nkz <= 0) continue;
+            const size_t e0 = compact_idx<N>(0, kyis, 2 * qs, 0);
+            for (int c = 0; c < (STAGE > 0 ? 6 : 3); ++c) {
+                const cplx<T>* base = c < 3 ? u0 + c * CS : acc + (c - 3) * CS;
+                const uintptr_t b0 = (uintptr_t)(base + e0);
+                const uintptr_t b1 = b0 + (uintptr_t)nkz * KK * sizeof(cplx<T>);
+                const uintptr_t a0 = (b0 + 15) & ~(uintptr_t)15, a1 = b1 & ~(uintptr_t)15;
+                if (a1 > a0) tma::prefetch_l2((const void*)a0, (uint32_t)(a1 - a0));
+            }
+        }
+    }
     auto st_at = [&](int s, int f, int kxi) -> Pair<T>& {
         return stage[((size_t)s * NF + f) * KK + kxi];
     };
