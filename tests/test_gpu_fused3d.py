@@ -147,3 +147,36 @@ def test_fused3d_tgv_512_fp32_one_step_vs_fp64(form):
     want = g.state_native()
     err = float((got.to(want.dtype) - want).abs().max() / want.abs().max())
     assert err < 1e-5, err
+
+
+@pytest.mark.parametrize("dtype,tol", [("float32", 1e-5), ("float64", 1e-12)])
+def test_fused3d_512_random_basdevant_one_step_vs_fp64(dtype, tol):
+    """n = 512 (one warp per transform in every pass) from a general state: the Taylor-Green
+    state has w = 0, so its products u w and v w vanish and the transforms that carry them
+    are not checked by it.  One step of the fused engine from a smooth random field against
+    the fp64 cuFFT engine from the same state."""
+    import torch
+
+    n = 512
+    cfg = Config(n=n, dim=3, nu=1e-3, dtype=dtype, form="basdevant")
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    phys = torch.randn((3, n, n, n), generator=gen, device="cuda", dtype=torch.float64)
+    ic = torch.fft.rfftn(phys, dim=(1, 2, 3))
+    del phys
+    k = torch.fft.fftfreq(n, 1.0 / n, device="cuda", dtype=torch.float64)
+    kz = torch.arange(n // 2 + 1, device="cuda", dtype=torch.float64)
+    ic *= torch.exp(-(k[:, None, None] ** 2 + k[None, :, None] ** 2 + kz[None, None, :] ** 2)
+                    / 200.0) * 1e-3
+    f = get(FUSED).make(cfg)
+    f.set_state(ic)
+    h = 0.5 * (2 * math.pi / n) / f.diag.max_velocity_sum(f.state_native())
+    f.step(h)
+    got = f.state_native().clone()
+    del f
+    torch.cuda.empty_cache()
+    g = get("b200").make(cfg.with_(dtype="float64"))
+    g.set_state(ic)
+    g.step(h)
+    want = g.state_native()
+    err = float((got.to(want.dtype) - want).abs().max() / want.abs().max())
+    assert err < tol, err
