@@ -68,6 +68,25 @@ def test_get_states_equals_get_state_of_each_member():
         assert np.array_equal(allst[i], ens.get_state(i)), i
 
 
+def test_set_states_twice_in_a_row_keeps_the_second():
+    """set_states stages each class through one pinned host buffer and copies it to the device
+    asynchronously: a second call right after the first waits for the first copy before it
+    overwrites the buffer, so the members hold the second states (compared with an ensemble
+    given only those)."""
+    from pyspectral_b200.ensemble import Ensemble
+
+    cfgs = _members("float32")
+    ics = _ics(cfgs)
+    second = [2.0 * a for a in ics]
+    ens = Ensemble(cfgs, autotune=False)
+    ens.set_states(ics)
+    ens.set_states(second)
+    ref = Ensemble(cfgs, autotune=False)
+    ref.set_states(second)
+    for i, (a, b) in enumerate(zip(ens.get_states(), ref.get_states())):
+        assert np.array_equal(a, b), i
+
+
 def test_batched_diagnostics_and_cfl_match_single_runs():
     from pyspectral_b200.ensemble import Ensemble
 
