@@ -407,7 +407,11 @@ template <typename T, int N, bool ROT>
 struct XPass {
     using D = Dims<N>;
     static constexpr int S = D::SEQ;
-    static constexpr int G = (S >= 2 || sizeof(T) == 8) ? 1 : 2;
+    // rotational form (six fields) at n = 512 in fp32: one kz pair per CTA and three CTAs per
+    // SM, which leaves the pass its registers (two pairs of 12 warps at two CTAs spill)
+    static constexpr bool ONE_PAIR_ROT = ROT && sizeof(T) == 4 && S == 1;
+    static constexpr int G = (S >= 2 || sizeof(T) == 8 || ONE_PAIR_ROT) ? 1 : 2;
+    static constexpr int MIN_BLOCKS = ONE_PAIR_ROT ? 3 : 2;
     static constexpr int U = G * S;
     static constexpr int WARPS = G * nslot<ROT>();
     static constexpr int THREADS = WARPS * 32;
@@ -428,7 +432,7 @@ __device__ __forceinline__ size_t compact_idx(int c, int kyi, int kz, int kxi) {
 }
 
 template <typename T, int N, bool ROT, int STAGE>
-__global__ void __launch_bounds__(XPass<T, N, ROT>::THREADS, 2) k3_x(
+__global__ void __launch_bounds__(XPass<T, N, ROT>::THREADS, XPass<T, N, ROT>::MIN_BLOCKS) k3_x(
     Pair<T>* __restrict__ Bs, cplx<T>* __restrict__ u0, cplx<T>* __restrict__ acc,
     const T* __restrict__ tab, const StepParams<T>* __restrict__ P,
     const cplx<T>* __restrict__ tw) {
