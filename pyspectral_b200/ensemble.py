@@ -338,7 +338,9 @@ class Ensemble:
 
     # ------------------------------------------------------------------ state
     def set_states(self, states: Sequence[np.ndarray]) -> None:
-        """Load every member's spectral state (host arrays, NumPy r2c layout)."""
+        """Load every member's spectral state (host arrays, NumPy r2c layout).  Each size class
+        goes through one pinned host buffer of its state's size, kept for the ensemble's
+        lifetime and shared with get_states."""
         if len(states) != len(self.members):
             raise ValueError("one state per member")
         for i, a in enumerate(states):
