@@ -238,15 +238,17 @@ __global__ void __launch_bounds__(RowPairs<N>::THREADS) k_row_max(const Pair<T>*
     const int p = blockIdx.x * F::B + sub;
     X += blockIdx.y * x_stride;
     umax += 2 * blockIdx.y;
+    static_assert(RI == 16, "slot m holds k = k0 + m n/16");
+    const int k0 = spec_base<N>(t);  // see seq_fft; the maximum needs no sample order
     Pair<T> v[16];
 #pragma unroll
     for (int g = 0; g < 16 / RI; ++g)
 #pragma unroll
         for (int m = 0; m < RI; ++m) {
-            const int k = in_pos<N, RI>(t, g, m);
+            const int k = in_pos<N, RI>(k0, g, m);
             v[g * RI + m] = Pair<T>{row_input<T, N>(X, p, k, kc, 0), row_input<T, N>(X, p, k, kc, 1)};
         }
-    block_fft<N, true>(v, sm, t, tw);
+    seq_fft<N, true>(v, sm, t, tw);
     double mu = 0.0, mv = 0.0;
     bool nan_u = false, nan_v = false;
 #pragma unroll
