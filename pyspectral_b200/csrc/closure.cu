@@ -98,17 +98,42 @@ __device__ __forceinline__ void issue(uint32_t d, uint32_t a, int a_mn, int a_C,
 }
 
 // Stages the 3 x 5 x 132 stencil rows of one tile (periodic wrap, n a power of two), scaled.
-__device__ __forceinline__ void stage_stencil(float* sSt, const float* f0, size_t fstride,
-                                              int rstride, int n, int row, int y0,
+// A tile's stencil in two halves: stencil_load issues all of a thread's loads into registers
+// (one memory latency per tile, and none at all when they are issued a tile ahead);
+// stencil_store scales them into shared memory.
+template <int THREADS>
+constexpr int stencil_per_thread() { return (kStencil + THREADS - 1) / THREADS; }
+
+template <int THREADS>
+__device__ __forceinline__ void stencil_load(float (&v)[stencil_per_thread<THREADS>()],
+                                             const float* f0, size_t fstride, int rstride, int n,
+                                             int row, int y0) {
+#pragma unroll
+    for (int i = 0; i < stencil_per_thread<THREADS>(); ++i) {
+        const int e = threadIdx.x + i * THREADS;
+        if (e < kStencil) {
+            const int f = e / (5 * kSpan);
+            const int r = (e / kSpan) % 5;
+            const int c = e % kSpan;
+            const int xr = (row + r - kHalo) & (n - 1);
+            const int yc = (y0 + c - kHalo) & (n - 1);
+            v[i] = f0[(size_t)f * fstride + (size_t)xr * rstride + yc];
+        }
+    }
+}
+
+template <int THREADS>
+__device__ __forceinline__ void stencil_store(float* sSt,
+                                              const float (&v)[stencil_per_thread<THREADS>()],
                                               const Consts& cc) {
-    for (int e = threadIdx.x; e < kStencil; e += blockDim.x) {
-        const int f = e / (5 * kSpan);
-        const int r = (e / kSpan) % 5;
-        const int c = e % kSpan;
-        const int xr = (row + r - kHalo) & (n - 1);
-        const int yc = (y0 + c - kHalo) & (n - 1);
-        const float sc = f == 0 ? cc.inscale[0] : (f == 1 ? cc.inscale[1] : cc.inscale[2]);
-        sSt[e] = f0[(size_t)f * fstride + (size_t)xr * rstride + yc] * sc;
+#pragma unroll
+    for (int i = 0; i < stencil_per_thread<THREADS>(); ++i) {
+        const int e = threadIdx.x + i * THREADS;
+        if (e < kStencil) {
+            const int f = e / (5 * kSpan);
+            const float sc = f == 0 ? cc.inscale[0] : (f == 1 ? cc.inscale[1] : cc.inscale[2]);
+            sSt[e] = v[i] * sc;
+        }
     }
 }
 
@@ -334,12 +359,21 @@ __global__ void __launch_bounds__(128, 1)
     uint32_t phase = 0;
     bool ok = true, first = true;
     float loss = 0.f;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const TilePick pk = pick_tile(seed, step, tile, count, n);
+    // the stencil and target of the CTA's next tile are loaded while the current one computes
+    float nxt[stencil_per_thread<128>()];
+    float nxt_target = 0.f;
+    auto load_tile = [&](int tl) {
+        const TilePick pk = pick_tile(seed, step, tl, count, n);
         const int y0 = pk.seg * kTile;
         const float* snap = bank + (size_t)pk.snap * 4 * n * n;
-        stage_stencil(sSt, snap, (size_t)n * n, n, n, pk.row, y0, cc);
-        const float target = snap[3 * (size_t)n * n + (size_t)pk.row * n + y0 + t] * cc.inv_outscale;
+        nxt_target = snap[3 * (size_t)n * n + (size_t)pk.row * n + y0 + t];
+        stencil_load<128>(nxt, snap, (size_t)n * n, n, n, pk.row, y0);
+    };
+    if (blockIdx.x < ntiles) load_tile(blockIdx.x);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        stencil_store<128>(sSt, nxt, cc);
+        const float target = nxt_target * cc.inv_outscale;
+        if (tile + (int)gridDim.x < ntiles) load_tile(tile + gridDim.x);
         __syncthreads();
         build_x(sX, sSt, t);
 
