@@ -340,6 +340,18 @@ __global__ void __launch_bounds__(128, 1)
     const Consts cc = *ccp;
     const int64_t step = step_override >= 0 ? step_override : (int64_t)*step_dev;
 
+    // the stencil and target of the CTA's next tile are loaded while the current one computes
+    // (the first tile's while the weights are staged)
+    float nxt[stencil_per_thread<128>()];
+    float nxt_target = 0.f;
+    auto load_tile = [&](int tl) {
+        const TilePick pk = pick_tile(seed, step, tl, count, n);
+        const int y0 = pk.seg * kTile;
+        const float* snap = bank + (size_t)pk.snap * 4 * n * n;
+        nxt_target = snap[3 * (size_t)n * n + (size_t)pk.row * n + y0 + t];
+        stencil_load<128>(nxt, snap, (size_t)n * n, n, n, pk.row, y0);
+    };
+    if (blockIdx.x < ntiles) load_tile(blockIdx.x);
     stage_weights<128>(sW, wb);
     if (t < kK) sW4[t] = params[kLayers * kWsz + t];
     for (int i = t; i < 4 * kK; i += blockDim.x) sDW4[i] = 0.f;  // one row per warp
@@ -359,17 +371,6 @@ __global__ void __launch_bounds__(128, 1)
     uint32_t phase = 0;
     bool ok = true, first = true;
     float loss = 0.f;
-    // the stencil and target of the CTA's next tile are loaded while the current one computes
-    float nxt[stencil_per_thread<128>()];
-    float nxt_target = 0.f;
-    auto load_tile = [&](int tl) {
-        const TilePick pk = pick_tile(seed, step, tl, count, n);
-        const int y0 = pk.seg * kTile;
-        const float* snap = bank + (size_t)pk.snap * 4 * n * n;
-        nxt_target = snap[3 * (size_t)n * n + (size_t)pk.row * n + y0 + t];
-        stencil_load<128>(nxt, snap, (size_t)n * n, n, n, pk.row, y0);
-    };
-    if (blockIdx.x < ntiles) load_tile(blockIdx.x);
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         stencil_store<128>(sSt, nxt, cc);
         const float target = nxt_target * cc.inv_outscale;
